@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FFT library on its headline workload.
+
+Workload (one "step"): the batched 1D real round trip — R2C forward then
+C2R inverse — for N in {1000, 2187, 6000, 2^20}, float32, each N with a
+batch that makes ~1 GiB of real input (268435, 122741, 44739, 256 rows),
+inputs U[-1, 1] from seed 20261029 + N.  Inputs (1 GiB per size) are far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+Metric: GFLOP/s counting 5 N log2 N per real transform (R2C and C2R each),
+whole job over all ranks; `gflops_2_5nlogn` gives the 2.5 N log2 N count.
+`value` times the library's kernels on HBM-resident inputs; `e2e` times
+the same work through the C ABI from pinned host buffers, with every
+host->device input copy and device->host result copy inside the region.
+
+`--impl reference` times the CPU implementation of the reference's
+algorithm (the oracle's C restatement of its Stockham / real pack
+arithmetic, oracle/stockham.c) on the host cores, on bounded samples of
+the same workload, and prints the same JSON line with "impl": "reference".
+
+Multi-GPU (`torchrun --nproc-per-node N bench.py --gpus N`): the transforms
+are independent, so every rank runs its own replica of the workload
+(replicas only, weak scaling); timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SIZES = [(1000, 268435), (2187, 122741), (6000, 44739), (1 << 20, 256)]
+SEED = 20261029
+METRIC = "FFT GFLOP/s & %HBM roofline at <=1e-6 rel err (R2C+C2R round trip)"
+
+
+def flops_real(n: int, rows: int, coef: float = 5.0) -> float:
+    return coef * n * math.log2(n) * rows
+
+
+def bytes_real(n: int, rows: int) -> int:
+    return rows * (4 * n + 8 * (n // 2 + 1))
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:8]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        sm = sorted(r[0] for r in rows)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+# --------------------------------------------------------------- CPU arms
+def cpu_sample(seconds_per_size: float, threads: int, steps: int = 1) -> dict:
+    """Round trip of the oracle's C restatement on bounded row samples."""
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    total_flops = 0.0
+    total_time = 0.0
+    sample = []
+    for n, rows in SIZES:
+        chunk = max(1, min(rows, int(4e6 // n) * threads // max(threads, 1)))
+        rng = np.random.default_rng(SEED + n)
+        x = rng.uniform(-1, 1, (chunk, n)).astype(np.float32)
+        done = 0
+        t0 = time.perf_counter()
+        while True:
+            spec = O.stockham(O.R2C, O.FORWARD, x, n)
+            O.stockham(O.C2R, O.INVERSE, spec, n)
+            done += chunk
+            el = time.perf_counter() - t0
+            if el >= seconds_per_size * steps or done >= rows:
+                break
+        total_time += el
+        total_flops += 2 * flops_real(n, done)
+        sample.append(f"N={n}: {done} of {rows} rows")
+    return {"gflops": total_flops / total_time / 1e9, "seconds": total_time, "sample": "; ".join(sample)}
+
+
+def run_reference(args) -> None:
+    from oracle import oracle as O
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(0.05, threads)
+    t0 = time.perf_counter()
+    res = cpu_sample(args.ref_seconds, threads, steps=args.steps)
+    wall = time.perf_counter() - t0
+    info = O.cpu_info()
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": round(res["gflops"], 3), "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic U[-1,1], seed 20261029+N",
+        "config": {"workload": "1D R2C->C2R round trip, N in {1000,2187,6000,2^20}, ~1 GiB input per N",
+                   "sizes": [list(s) for s in SIZES], "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(res["gflops"], 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "cpu": info["model"],
+                         "sample": res["sample"] + " (C restatement of the reference's Stockham arithmetic, "
+                                                   "oracle/stockham.c, rows split over all host threads)"},
+        "e2e": {"value": round(res["gflops"], 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args) -> None:
+    import torch
+
+    from sip_b200 import _lib as L
+    from sip_b200.fft import FftHandle, check
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    sizes = SIZES if not args.quick else [(n, max(2, b // 64)) for n, b in SIZES]
+    stream = torch.cuda.Stream(device=dev)
+
+    plans = []
+    for n, rows in sizes:
+        g = torch.Generator(device=dev)
+        g.manual_seed(SEED + n)
+        x = torch.rand((rows, n), generator=g, device=dev, dtype=torch.float32).mul_(2).sub_(1)
+        spec = torch.empty((rows, n // 2 + 1), dtype=torch.complex64, device=dev)
+        y = torch.empty((rows, n), dtype=torch.float32, device=dev)
+        hr, hc = FftHandle(), FftHandle()
+        check(hr.make_plan_1d(n, L.ASCEND_FFT_R2C, L.ASCEND_FFT_FORWARD, rows), "plan r2c")
+        check(hc.make_plan_1d(n, L.ASCEND_FFT_C2R, L.ASCEND_FFT_INVERSE, rows), "plan c2r")
+        for h in (hr, hc):
+            h.bind_workspace(dev)
+            check(h.set_stream(stream), "set stream")
+        kr = len(hr.describe()["steps"])
+        kc = len(hc.describe()["steps"])
+        plans.append(dict(n=n, rows=rows, x=x, spec=spec, y=y, hr=hr, hc=hc, kernels=(kr, kc)))
+    torch.cuda.synchronize()
+
+    def step(events=None):
+        for i, p in enumerate(plans):
+            if events is not None:
+                events[i][0].record(stream)
+            check(p["hr"].exec_raw(p["x"].data_ptr(), p["spec"].data_ptr()), "exec r2c")
+            if events is not None:
+                events[i][1].record(stream)
+            check(p["hc"].exec_raw(p["spec"].data_ptr(), p["y"].data_ptr()), "exec c2r")
+            if events is not None:
+                events[i][2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in plans] for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t_start.record(stream)
+        for s in range(args.steps):
+            step(ev[s])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # per-exec durations (ms), averaged over steps
+    per = []
+    for i, p in enumerate(plans):
+        r2c = np.mean([ev[s][i][0].elapsed_time(ev[s][i][1]) for s in range(args.steps)])
+        c2r = np.mean([ev[s][i][1].elapsed_time(ev[s][i][2]) for s in range(args.steps)])
+        per.append((p, r2c, c2r))
+
+    # parity on a seeded row sample of every size (FP64 oracle) and round trip
+    from oracle import oracle as O
+
+    parity = {}
+    for p in plans:
+        n, rows = p["n"], p["rows"]
+        idx = np.unique(np.linspace(0, rows - 1, min(rows, 16)).astype(np.int64))
+        it = torch.from_numpy(idx).to(dev)
+        xs = p["x"].index_select(0, it).cpu().numpy()
+        ss = p["spec"].index_select(0, it).cpu().numpy()
+        ys = p["y"].index_select(0, it).cpu().numpy()
+        e_r2c = O.rel_l2(ss, O.fp64(O.R2C, O.FORWARD, xs, [n]))
+        e_rt = O.rel_l2(ys / n, xs)
+        parity[str(n)] = {"r2c_rel_l2": float(f"{e_r2c:.3e}"), "roundtrip_rel_l2": float(f"{e_rt:.3e}")}
+
+    launches_per_step = sum(sum(p["kernels"]) for p in plans)
+    step_flops = sum(2 * flops_real(p["n"], p["rows"]) for p in plans)
+    step_flops25 = sum(2 * flops_real(p["n"], p["rows"], 2.5) for p in plans)
+    step_bytes = sum(2 * bytes_real(p["n"], p["rows"]) for p in plans)
+    ms_per_step = total_ms / args.steps
+    value = world * step_flops / (ms_per_step * 1e-3) / 1e9
+
+    # roofline of the dominant single-kernel exec
+    peak, peak_kind = load_peaks()
+    cands = []
+    for p, r2c, c2r in per:
+        for name, ms, k in (("r2c", r2c, p["kernels"][0]), ("c2r", c2r, p["kernels"][1])):
+            gbs = bytes_real(p["n"], p["rows"]) / (ms * 1e-3) / 1e9
+            cands.append(dict(exec=f"{name} N={p['n']} rows={p['rows']}", kernels=k, ms=float(f"{ms:.4f}"),
+                              gbs=round(gbs, 1), frac=round(gbs / peak, 4),
+                              bytes=bytes_real(p["n"], p["rows"])))
+    single = [c for c in cands if c["kernels"] == 1]
+    dom = max(single or cands, key=lambda c: c["ms"])
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(dom["exec"].split(" rows")[0])
+
+    # end to end through the C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host_in = [p["x"].cpu().pin_memory() for p in plans]
+        host_out = [torch.empty(p["y"].shape, dtype=torch.float32).pin_memory() for p in plans]
+        dev_in = [torch.empty_like(p["x"]) for p in plans]
+        ke = max(1, min(args.steps, 3))
+
+        def e2e_step():
+            for i, p in enumerate(plans):
+                with torch.cuda.stream(stream):
+                    dev_in[i].copy_(host_in[i], non_blocking=True)
+                check(p["hr"].exec_raw(dev_in[i].data_ptr(), p["spec"].data_ptr()), "exec r2c")
+                check(p["hc"].exec_raw(p["spec"].data_ptr(), p["y"].data_ptr()), "exec c2r")
+                with torch.cuda.stream(stream):
+                    host_out[i].copy_(p["y"], non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ke):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1) / ke
+        if dist:
+            t = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        assert np.allclose(host_out[0][:2].numpy() / plans[0]["n"], host_in[0][:2].numpy(), atol=1e-5)
+        hb = sum(t.numel() * 4 for t in host_in)
+        db = sum(t.numel() * 4 for t in host_out)
+        e2e = {"value": round(world * step_flops / (e_ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+               "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
+               "steps": ke}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        res = cpu_sample(args.cpu_seconds, threads)
+        cpu = {"value": round(res["gflops"], 3), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+               "cpu": O.cpu_info()["model"],
+               "sample": res["sample"] + " (oracle/stockham.c, the C restatement of the reference's arithmetic)"}
+
+    if dist:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic U[-1,1] float32, seed 20261029+N, generated on the device",
+            "config": {"workload": "1D R2C->C2R round trip, N in {1000,2187,6000,2^20}, ~1 GiB input per N",
+                       "sizes": [[p["n"], p["rows"]] for p in plans], "parallelism": f"replicas x{world}",
+                       "l2": "inputs 1 GiB per size (> 126 MB L2), no flush"},
+            "gflops_2_5nlogn": round(world * step_flops25 / (ms_per_step * 1e-3) / 1e9, 3),
+            "hbm_gbs_step": round(world * step_bytes / (ms_per_step * 1e-3) / 1e9, 1),
+            "roofline": {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
+                         "traffic": traffic, "kernel": dom["exec"], "algorithmic_bytes": dom["bytes"],
+                         "peak_kind": peak_kind},
+            "execs": cands,
+            "parity": parity,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    for p in plans:
+        p["hr"].destroy()
+        p["hc"].destroy()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="1/64 of the batch (debugging only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")
+    ap.add_argument("--ref-seconds", type=float, default=1.5, help="reference arm seconds per size per step")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+"""Build recipe of the B200 FFT library.
+
+Compiles the CUDA kernels for sm_100a and the host C++ into the in-tree
+shared library ``sip_b200/libsip_fft.so`` (the C ABI of include/fft_api.h
+and include/sip_fft_ext.h).  Objects are cached under ``sip_b200/_build``
+and rebuilt when any source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libsip_fft.so"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+          "-I", str(ROOT / "include"), "-I", str(CSRC)]
+
+# (source, extra defines, object name)
+UNITS = [
+    ("tile_inst.cu", ["-DSIP_INST_SIGN=-1", "-DSIP_INST_E=16"], "tile_fwd_e16.o"),
+    ("tile_inst.cu", ["-DSIP_INST_SIGN=-1", "-DSIP_INST_E=32"], "tile_fwd_e32.o"),
+    ("tile_inst.cu", ["-DSIP_INST_SIGN=1", "-DSIP_INST_E=16"], "tile_inv_e16.o"),
+    ("tile_inst.cu", ["-DSIP_INST_SIGN=1", "-DSIP_INST_E=32"], "tile_inv_e32.o"),
+    ("tile_kernels.cu", [], "tile_kernels.o"),
+    ("twiddle.cu", [], "twiddle.o"),
+    ("real_kernels.cu", [], "real_kernels.o"),
+    ("plan.cpp", [], "plan.o"),
+    ("device.cpp", [], "device.o"),
+    ("api.cpp", [], "api.o"),
+    ("acl_tensor.cpp", [], "acl_tensor.o"),
+]
+
+
+def _newest_header() -> float:
+    heads = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").rglob("*.h"))
+    return max((h.stat().st_mtime for h in heads), default=0.0)
+
+
+def _compile(src: str, defs: list[str], obj: str, head_mtime: float, verbose: bool) -> str:
+    out = BUILD / obj
+    s = CSRC / src
+    if out.exists() and out.stat().st_mtime >= max(s.stat().st_mtime, head_mtime):
+        return f"up to date {obj}"
+    cmd = [NVCC, *ARCH, *COMMON, *defs, "-c", str(s), "-o", str(out)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src} {defs}:\n{r.stdout}\n{r.stderr}")
+    return f"built {obj}" + (("\n" + r.stderr) if verbose else "")
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    head = _newest_header()
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        futs = [ex.submit(_compile, s, d, o, head, verbose) for s, d, o in UNITS]
+        for f in futs:
+            msg = f.result()
+            if verbose:
+                print(msg)
+    objs = [str(BUILD / o) for _, _, o in UNITS]
+    newest = max(Path(o).stat().st_mtime for o in objs)
+    if not LIB.exists() or LIB.stat().st_mtime < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,456 @@
+// C ABI of the B200 FFT library (include/fft_api.h, include/sip_fft_ext.h).
+//
+// Validation order, status codes and the workspace protocol follow the
+// reference's public functions in core/fft/fft_api.cpp (asdFftCreate
+// :1047, asdFftSetStream :1067, asdFftMakePlan1D :1124, asdFftMakePlan2D
+// :1245, asdFftMakePlan3D :1292, asdFftGetWorkspaceSize :1339,
+// asdFftSetWorkspace :1361, asdFftSynchronize :1376, asdFftGetType :1392,
+// asdFftExecV2 :1446, tensor matching :1512-1750, asdFftExecC2C/C2R/R2C
+// :1752-1844).  Every call holds one process-wide mutex, as the reference's
+// fft_mtx does; no exception crosses the ABI.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "acl_tensor.h"
+#include "fft_api.h"
+#include "plan.h"
+#include "sip_fft_ext.h"
+
+using namespace AsdSip;
+using sipfft::FftPlan;
+using sipfft::PlanError;
+
+namespace {
+
+std::mutex g_mu;
+std::unordered_map<void*, std::unique_ptr<FftPlan>> g_plans;
+
+constexpr int64_t kMaxFftSize = int64_t(1) << 27;
+
+FftPlan* find_plan(asdFftHandle h) {
+    auto it = g_plans.find(h);
+    return it == g_plans.end() ? nullptr : it->second.get();
+}
+
+bool trace_enabled() {
+    const char* t = std::getenv("ASDSIP_FFT_PLAN_TRACE");
+    return t != nullptr && std::strcmp(t, "1") == 0;
+}
+
+bool device_present() {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+// Builds the kernel steps and, when a GPU is present, the device tables.
+// Any failure leaves the plan uninitialised; the reference reports plan
+// construction failures as INVALID_PARAM (fft_api.cpp:1181-1187).
+AspbStatus finish_plan(FftPlan& plan) {
+    try {
+        sipfft::build_steps(plan);
+        if (device_present()) sipfft::prepare_device(plan);
+    } catch (const std::exception& e) {
+        plan.steps.clear();
+        plan.resources_ready = false;
+        std::fprintf(stderr, "[sip_b200] make plan failed: %s\n", e.what());
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    plan.initialized = true;
+    if (trace_enabled()) std::fprintf(stderr, "ASDSIP_FFT_PLAN %s\n", sipfft::describe(plan).c_str());
+    return ACL_SUCCESS;
+}
+
+AspbStatus check_direction(asdFftDirection d) {
+    return (d == ASCEND_FFT_FORWARD || d == ASCEND_FFT_INVERSE) ? ACL_SUCCESS : ACL_ERROR_INVALID_PARAM;
+}
+
+// ---------------------------------------------------------- tensor match
+struct View {
+    std::vector<int64_t> dims;
+    aclDataType dtype = ACL_DT_UNDEFINED;
+    bool ok = false;
+};
+
+View view_of(const aclTensor* t) {
+    View v;
+    if (t == nullptr) return v;
+    int64_t* dims = nullptr;
+    uint64_t n = 0;
+    if (aclGetViewShape(t, &dims, &n) != 0) {
+        delete[] dims;
+        return v;
+    }
+    v.dims.assign(dims, dims + n);
+    delete[] dims;
+    if (aclGetDataType(t, &v.dtype) != 0) return v;
+    v.ok = true;
+    return v;
+}
+
+// Product of the leading dims [0, count) equals the plan's batch.
+bool leading_is_batch(const std::vector<int64_t>& dims, size_t count, int64_t batch) {
+    int64_t e = 1;
+    for (size_t i = 0; i < count; ++i) {
+        if (dims[i] <= 0 || e > batch / dims[i]) return false;
+        e *= dims[i];
+    }
+    return e == batch;
+}
+
+// Trailing dims equal the plan's sizes, the last one replaced by
+// last_override when >= 0; leading extent equals batch.
+bool match_shape(const FftPlan& p, const View& v, int64_t last_override) {
+    const size_t nd = p.sizes.size();
+    if (v.dims.size() < nd) return false;
+    const size_t lead = v.dims.size() - nd;
+    for (size_t i = 0; i < nd; ++i) {
+        int64_t want = p.sizes[i];
+        if (i == nd - 1 && last_override >= 0) want = last_override;
+        if (v.dims[lead + i] != want) return false;
+    }
+    return leading_is_batch(v.dims, lead, p.batch);
+}
+
+// Reference matchC2C_ (fft_api.cpp:1568-1618): 1D tensors have rank 2,
+// (batch, N); a batch-1 plan also accepts (N, 1).
+bool match_c2c(const FftPlan& p, const aclTensor* t) {
+    View v = view_of(t);
+    if (!v.ok || v.dtype != ACL_COMPLEX64) return false;
+    if (p.sizes.size() == 1) {
+        if (v.dims.size() != 2) return false;
+        if (p.batch == 1) return (v.dims[0] == 1 && v.dims[1] == p.sizes[0]) || (v.dims[0] == p.sizes[0] && v.dims[1] == 1);
+        return v.dims[0] == p.batch && v.dims[1] == p.sizes[0];
+    }
+    return match_shape(p, v, -1);
+}
+
+// Half-spectrum side (reference matchC2R_, fft_api.cpp:1620-1674).
+bool match_spectrum(const FftPlan& p, const aclTensor* t) {
+    View v = view_of(t);
+    if (!v.ok || v.dtype != ACL_COMPLEX64) return false;
+    return match_shape(p, v, p.sizes.back() / 2 + 1);
+}
+
+// Real side (reference matchR2C_, fft_api.cpp:1676-1718).
+bool match_real(const FftPlan& p, const aclTensor* t) {
+    View v = view_of(t);
+    if (!v.ok || v.dtype != ACL_FLOAT) return false;
+    return match_shape(p, v, -1);
+}
+
+// --------------------------------------------------------------- exec
+size_t operand_bytes(const FftPlan& p, bool input) {
+    int64_t rows = p.batch;
+    for (size_t i = 0; i + 1 < p.sizes.size(); ++i) rows *= p.sizes[i];
+    const int64_t n = p.sizes.back();
+    const size_t real_b = (size_t)(rows * n * 4);
+    const size_t spec_b = (size_t)(rows * (n / 2 + 1) * 8);
+    switch (p.type) {
+        case ASCEND_FFT_R2C: return input ? real_b : spec_b;
+        case ASCEND_FFT_C2R: return input ? spec_b : real_b;
+        default: return (size_t)(rows * n * 8);
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int want) {
+        if (want < 0) return;
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != want) cudaSetDevice(want);
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Reference asdFftExecV2 + CheckWorkspaceBinding (fft_api.cpp:1020-1032,
+// 1446-1511).
+AspbStatus exec_plan(FftPlan& p, const void* in, void* out) {
+    if (!p.initialized) return ACL_ERROR_INVALID_PARAM;
+    const bool ws_required = p.workspace_need > 0;
+    if (ws_required && p.workspace == nullptr) {
+        std::fprintf(stderr, "[sip_b200] workspace has not been set\n");
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    if (ws_required && p.workspace_recorded == 0) {
+        std::fprintf(stderr, "[sip_b200] call asdFftGetWorkspaceSize before exec\n");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (in == nullptr || out == nullptr) return ACL_ERROR_INTERNAL_ERROR;
+    // Input and output must be separate, or exactly aliased for C2C plans
+    // (every C2C plan reads a tile before it writes the same tile).
+    const char* ib = static_cast<const char*>(in);
+    const char* ob = static_cast<const char*>(out);
+    const size_t isz = operand_bytes(p, true), osz = operand_bytes(p, false);
+    const bool overlap = ib < ob + osz && ob < ib + isz;
+    if (overlap && !(ib == ob && p.type == ASCEND_FFT_C2C)) {
+        std::fprintf(stderr, "[sip_b200] input and output overlap\n");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    try {
+        if (!p.resources_ready) {
+            if (!device_present()) return ACL_ERROR_INTERNAL_ERROR;
+            sipfft::prepare_device(p);
+        }
+        DeviceGuard g(p.device);
+        sipfft::launch_steps(p, in, out, p.workspace);
+    } catch (const PlanError& e) {
+        std::fprintf(stderr, "[sip_b200] exec failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] exec failed: %s\n", e.what());
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    return ACL_SUCCESS;
+}
+
+AspbStatus exec_tensors(asdFftHandle handle, asdFftType want, const aclTensor* input, const aclTensor* output) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || !p->initialized) return ACL_ERROR_INVALID_PARAM;
+    if (p->type != want) return ACL_ERROR_INVALID_PARAM;
+    bool ok_in = false, ok_out = false;
+    switch (want) {
+        case ASCEND_FFT_C2C:
+            ok_in = match_c2c(*p, input);
+            ok_out = match_c2c(*p, output);
+            break;
+        case ASCEND_FFT_R2C:
+            ok_in = match_real(*p, input);
+            ok_out = match_spectrum(*p, output);
+            break;
+        case ASCEND_FFT_C2R:
+            ok_in = match_spectrum(*p, input);
+            ok_out = match_real(*p, output);
+            break;
+        default:
+            break;
+    }
+    if (!ok_in || !ok_out) {
+        std::fprintf(stderr, "[sip_b200] tensor does not match the plan\n");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    return exec_plan(*p, aclGetTensorData(input), aclGetTensorData(output));
+}
+
+}  // namespace
+
+extern "C" {
+
+namespace AsdSip {
+
+AspbStatus asdFftCreate(asdFftHandle& handle) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    try {
+        auto plan = std::make_unique<FftPlan>();
+        void* key = plan.get();
+        g_plans.emplace(key, std::move(plan));
+        handle = key;
+    } catch (const std::exception&) {
+        handle = nullptr;
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftSetStream(asdFftHandle handle, void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (stream == nullptr) return ACL_ERROR_INVALID_PARAM;
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    p->stream = stream;
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftMakePlan1D(asdFftHandle handle, int64_t fftSize, asdFftType fftType, asdFftDirection direction,
+                            int64_t batchSize, asdFft1dDimType dimType) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    if (fftSize <= 0 || fftSize > kMaxFftSize) return ACL_ERROR_INVALID_PARAM;
+    if (batchSize <= 0 || batchSize > (int64_t)std::numeric_limits<int32_t>::max()) return ACL_ERROR_INVALID_PARAM;
+    if (fftType != ASCEND_FFT_C2C && fftType != ASCEND_FFT_C2R && fftType != ASCEND_FFT_R2C &&
+        fftType != ASCEND_FFT_C2C_SEP)
+        return ACL_ERROR_INVALID_PARAM;
+    if (check_direction(direction) != ACL_SUCCESS) return ACL_ERROR_INVALID_PARAM;
+    if (p->initialized) return ACL_ERROR_INVALID_PARAM;
+    if (dimType != ASCEND_FFT_HORIZONTAL && dimType != ASCEND_FFT_VERTICAL) return ACL_ERROR_INVALID_PARAM;
+    // Vertical batches are rejected as on the reference's Ascend 950 route
+    // (fft_api.cpp:1111-1116); strided layouts are not part of this ABI.
+    if (dimType == ASCEND_FFT_VERTICAL && batchSize > 1) return ACL_ERROR_API_NOT_SUPPORT;
+    p->type = fftType;
+    p->direction = direction;
+    p->sizes = {fftSize};
+    p->batch = batchSize;
+    p->vertical = dimType == ASCEND_FFT_VERTICAL;
+    if (fftType == ASCEND_FFT_C2C_SEP) p->type = ASCEND_FFT_C2C_SEP;
+    return finish_plan(*p);
+}
+
+AspbStatus asdFftIstftMakePlan(asdFftHandle handle, const aclTensor* input, const int64_t nFft,
+                               const int64_t hopLengthOpt, const int64_t winLengthOpt, const bool center,
+                               const bool normalized, const bool onesidedOpt, int64_t lengthOpt,
+                               const bool returnComplex) {
+    (void)handle; (void)input; (void)nFft; (void)hopLengthOpt; (void)winLengthOpt; (void)center;
+    (void)normalized; (void)onesidedOpt; (void)lengthOpt; (void)returnComplex;
+    return ACL_ERROR_API_NOT_SUPPORT;
+}
+
+AspbStatus asdFftExecC2C(asdFftHandle handle, const aclTensor* input, const aclTensor* output) {
+    return exec_tensors(handle, ASCEND_FFT_C2C, input, output);
+}
+
+AspbStatus asdFftExecC2CSeparated(asdFftHandle handle, const aclTensor* inputReal, const aclTensor* inputImag,
+                                  const aclTensor* outputReal, const aclTensor* outputImag) {
+    (void)inputReal; (void)inputImag; (void)outputReal; (void)outputImag;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (find_plan(handle) == nullptr) return ACL_ERROR_INVALID_PARAM;
+    return ACL_ERROR_API_NOT_SUPPORT;
+}
+
+AspbStatus asdFftExecC2R(asdFftHandle handle, const aclTensor* input, const aclTensor* output) {
+    return exec_tensors(handle, ASCEND_FFT_C2R, input, output);
+}
+
+AspbStatus asdFftExecR2C(asdFftHandle handle, const aclTensor* input, const aclTensor* output) {
+    return exec_tensors(handle, ASCEND_FFT_R2C, input, output);
+}
+
+AspbStatus asdFftExecIstft(asdFftHandle handle, const aclTensor* input, const aclTensor* windowOpt,
+                           const aclTensor* output) {
+    (void)handle; (void)input; (void)windowOpt; (void)output;
+    return ACL_ERROR_API_NOT_SUPPORT;
+}
+
+AspbStatus asdFftDestroy(asdFftHandle handle) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_plans.find(handle);
+    if (it == g_plans.end()) return ACL_ERROR_INVALID_PARAM;
+    g_plans.erase(it);
+    return ACL_SUCCESS;
+}
+
+namespace {
+AspbStatus common_check(asdFftHandle handle, std::initializer_list<int64_t> sizes, int64_t batch) {
+    if (find_plan(handle) == nullptr) return ACL_ERROR_INVALID_PARAM;
+    for (int64_t s : sizes)
+        if (s <= 0 || s > kMaxFftSize) return ACL_ERROR_INVALID_PARAM;
+    if (batch <= 0) return ACL_ERROR_INVALID_PARAM;
+    return ACL_SUCCESS;
+}
+}  // namespace
+
+AspbStatus asdFftMakePlan2D(asdFftHandle handle, int64_t fftSizeX, int64_t fftSizeY, asdFftType fftType,
+                            asdFftDirection direction, int32_t batchSize) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    AspbStatus st = common_check(handle, {fftSizeX, fftSizeY}, batchSize);
+    if (st != ACL_SUCCESS) return st;
+    if (fftType != ASCEND_FFT_C2C && fftType != ASCEND_FFT_C2R && fftType != ASCEND_FFT_R2C)
+        return ACL_ERROR_INVALID_PARAM;
+    if (check_direction(direction) != ACL_SUCCESS) return ACL_ERROR_INVALID_PARAM;
+    FftPlan* p = find_plan(handle);
+    if (p->initialized) return ACL_ERROR_INVALID_PARAM;
+    p->type = fftType;
+    p->direction = direction;
+    p->sizes = {fftSizeX, fftSizeY};
+    p->batch = batchSize;
+    return finish_plan(*p);
+}
+
+AspbStatus asdFftMakePlan3D(asdFftHandle handle, int64_t fftSizeX, int64_t fftSizeY, int64_t fftSizeZ,
+                            asdFftType fftType, asdFftDirection direction, int32_t batchSize) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    AspbStatus st = common_check(handle, {fftSizeX, fftSizeY, fftSizeZ}, batchSize);
+    if (st != ACL_SUCCESS) return st;
+    if (fftType != ASCEND_FFT_C2C && fftType != ASCEND_FFT_C2R && fftType != ASCEND_FFT_R2C &&
+        fftType != ASCEND_FFT_C2C_SEP)
+        return ACL_ERROR_INVALID_PARAM;
+    if (check_direction(direction) != ACL_SUCCESS) return ACL_ERROR_INVALID_PARAM;
+    FftPlan* p = find_plan(handle);
+    if (p->initialized) return ACL_ERROR_INVALID_PARAM;
+    p->type = fftType;
+    p->direction = direction;
+    p->sizes = {fftSizeX, fftSizeY, fftSizeZ};
+    p->batch = batchSize;
+    return finish_plan(*p);
+}
+
+AspbStatus asdFftGetWorkspaceSize(asdFftHandle handle, size_t& workspaceSize) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    workspaceSize = p->workspace_need;
+    p->workspace_recorded = p->workspace_need;
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftSetWorkspace(asdFftHandle handle, void* workspace) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    p->workspace = workspace;
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftSynchronize(asdFftHandle handle) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INTERNAL_ERROR;
+    if (cudaStreamSynchronize(static_cast<cudaStream_t>(p->stream)) != cudaSuccess) return ACL_ERROR_INTERNAL_ERROR;
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftGetType(asdFftHandle handle, asdFftType& fftType) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INTERNAL_ERROR;
+    fftType = p->type;
+    return ACL_SUCCESS;
+}
+
+AspbStatus asdFftShift(int64_t row, int64_t col, int64_t batch, int64_t dist, const aclTensor* input,
+                       aclTensor* output, void* stream, void* workspace) {
+    (void)row; (void)col; (void)batch; (void)dist; (void)input; (void)output; (void)stream; (void)workspace;
+    return ACL_ERROR_API_NOT_SUPPORT;
+}
+
+AspbStatus asdIfftShift(int64_t row, int64_t col, int64_t batch, int64_t dist, double scale, const aclTensor* input,
+                        aclTensor* output, void* stream, void* workspace) {
+    (void)row; (void)col; (void)batch; (void)dist; (void)scale; (void)input; (void)output; (void)stream;
+    (void)workspace;
+    return ACL_ERROR_API_NOT_SUPPORT;
+}
+
+}  // namespace AsdSip
+
+AspbStatus sipFftExecRaw(asdFftHandle handle, const void* input, void* output) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    return exec_plan(*p, input, output);
+}
+
+AspbStatus sipFftDescribePlan(asdFftHandle handle, char* buf, size_t cap, size_t* needed) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    const std::string s = sipfft::describe(*p);
+    if (needed != nullptr) *needed = s.size() + 1;
+    if (buf != nullptr && cap > 0) {
+        const size_t n = s.size() < cap - 1 ? s.size() : cap - 1;
+        std::memcpy(buf, s.data(), n);
+        buf[n] = '\0';
+    }
+    return ACL_SUCCESS;
+}
+
+const char* sipFftVersion(void) { return "sip_b200-fft 0.1.0"; }
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// Device resources of plans and step launching.
+//
+// Twiddle tables are cached per (device, kind, parameters) through
+// weak_ptr, so plans of the same length share one device copy and the
+// copy is freed with its last plan (the reference's FFTensorCache,
+// core/fft/utils/fftensor_cache.cpp:82-101).
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <tuple>
+
+#include "plan.h"
+
+namespace sipfft {
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct TableKey {
+    int device;
+    int kind;  // 0 stockham, 1 roots
+    long long a, b;
+    std::vector<int> radices;
+    bool operator<(const TableKey& o) const {
+        return std::tie(device, kind, a, b, radices) < std::tie(o.device, o.kind, o.a, o.b, o.radices);
+    }
+};
+
+std::mutex g_table_mu;
+std::map<TableKey, std::weak_ptr<DeviceBuf>> g_tables;
+
+BufPtr alloc_buf(size_t bytes, int device) {
+    auto b = std::make_shared<DeviceBuf>();
+    b->device = device;
+    b->bytes = bytes;
+    if (bytes > 0) check(cudaMalloc(&b->ptr, bytes), "cudaMalloc");
+    return b;
+}
+
+// Runs `gen` on a private non-blocking stream and waits for it.
+template <class F>
+void run_sync(F gen) {
+    cudaStream_t s = nullptr;
+    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaError_t e = gen(s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    check(e, "table generation");
+}
+
+BufPtr stockham_table(int device, const PlanDev& pd, const std::vector<int>& radices) {
+    int entries = 0;
+    for (int i = 0; i < pd.npass; ++i)
+        if (pd.pass[i].L > 1) entries = pd.pass[i].tw + pd.pass[i].L * (pd.pass[i].R - 1);
+    TableKey key{device, 0, pd.N, 0, radices};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    BufPtr b = alloc_buf((size_t)std::max(entries, 1) * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_stockham_twiddles(static_cast<float2*>(b->ptr), pd, entries, s); });
+    g_tables[key] = b;
+    return b;
+}
+
+BufPtr root_table(int device, long long n, long long count) {
+    TableKey key{device, 1, n, count, {}};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    BufPtr b = alloc_buf((size_t)count * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_root_twiddles(static_cast<float2*>(b->ptr), n, count, s); });
+    g_tables[key] = b;
+    return b;
+}
+
+}  // namespace
+
+void prepare_device(FftPlan& plan) {
+    int device = -1;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    for (Step& st : plan.steps) {
+        if (st.tw2_kind == 1) st.tw2 = root_table(device, st.tw2_n, st.tw2_count);
+        if (st.kind != StepKind::Tile) {
+            st.real.tw = static_cast<const float2*>(st.tw2->ptr);
+            continue;
+        }
+        st.tw = stockham_table(device, st.host_plan, st.radices);
+        st.plan_dev = alloc_buf(sizeof(PlanDev), device);
+        check(cudaMemcpy(st.plan_dev->ptr, &st.host_plan, sizeof(PlanDev), cudaMemcpyHostToDevice), "cudaMemcpy");
+        st.L.args.plan = static_cast<const PlanDev*>(st.plan_dev->ptr);
+        st.L.args.tw = static_cast<const float2*>(st.tw->ptr);
+        st.L.args.tw2 = st.tw2 ? static_cast<const float2*>(st.tw2->ptr) : nullptr;
+        check(tile_prepare(st.L.sign, st.L.e, st.L.op, st.L.tw4, st.L.smem_bytes), "cudaFuncSetAttribute");
+    }
+    plan.device = device;
+    plan.resources_ready = true;
+}
+
+void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
+    cudaStream_t stream = static_cast<cudaStream_t>(plan.stream);
+    auto resolve = [&](Loc l, size_t off) -> char* {
+        char* base = nullptr;
+        switch (l) {
+            case Loc::In: base = const_cast<char*>(static_cast<const char*>(in)); break;
+            case Loc::Out: base = static_cast<char*>(out); break;
+            case Loc::Ws: base = static_cast<char*>(ws); break;
+        }
+        return base + off;
+    };
+    for (const Step& st : plan.steps) {
+        char* src = resolve(st.src, st.src_off);
+        char* dst = resolve(st.dst, st.dst_off);
+        if (st.kind == StepKind::Tile) {
+            check(tile_launch(st.L, src, dst, stream), "tile kernel launch");
+        } else {
+            RealPassArgs a = st.real;
+            a.src = reinterpret_cast<const float2*>(src);
+            a.dst = reinterpret_cast<float2*>(dst);
+            check(st.kind == StepKind::RealPost ? real_post(a, stream) : real_pre(a, stream), "real pass launch");
+        }
+    }
+}
+
+}  // namespace sipfft

@@ -1,0 +1,495 @@
+// Planner of the B200 FFT library.
+//
+// Replaces the reference's plan builder (core/fft/fft_api.cpp:662-992:
+// addFFTSteps / init2DSteps / init3DSteps with their per-axis core
+// routing and explicit last-two-axis transposes).  Here every axis pass is
+// one tile-kernel launch that reads its transforms in place through
+// strides, so a 2D transform is two HBM round trips and a 3D transform
+// three, with no transpose steps.  Lengths above one tile (16384 complex
+// points) use a two-pass four-step split N = N1 * N2.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <map>
+#include <sstream>
+#include <tuple>
+
+#include "real_kernels.h"
+
+namespace sipfft {
+
+using namespace AsdSip;
+
+DeviceBuf::~DeviceBuf() {
+    if (ptr == nullptr) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (device >= 0 && device != cur) cudaSetDevice(device);
+    cudaFree(ptr);
+    if (device >= 0 && device != cur && cur >= 0) cudaSetDevice(cur);
+}
+
+int64_t FftPlan::elements() const {
+    int64_t e = batch;
+    for (int64_t s : sizes) e *= s;
+    return e;
+}
+
+// ------------------------------------------------------------ radices
+namespace {
+
+struct RadixCost {
+    int r;
+    double cost;
+};
+
+// Cost of one pass: dominated by the shared-memory round trip (1.0); larger
+// radices pay a little for register pressure and prime radices for their
+// O(R^2) butterfly.
+double radix_cost(int r) {
+    double c = 1.0 + 0.002 * r;
+    if (r == 11 || r == 13 || r == 17 || r == 19) c += 0.2;
+    return c;
+}
+
+const int kRadixList[] = {32, 27, 25, 19, 17, 16, 15, 13, 11, 10, 9, 8, 7, 5, 4, 3, 2};
+
+}  // namespace
+
+std::vector<int> choose_radices(int n, int e) {
+    if (n == 1) return {};
+    const int maxr = e >= 32 ? 32 : 27;
+    std::map<int, std::pair<double, std::vector<int>>> memo;
+    std::function<std::pair<double, std::vector<int>>(int)> best = [&](int m) -> std::pair<double, std::vector<int>> {
+        if (m == 1) return {0.0, {}};
+        auto it = memo.find(m);
+        if (it != memo.end()) return it->second;
+        std::pair<double, std::vector<int>> res{1e30, {}};
+        for (int r : kRadixList) {
+            if (r > maxr || m % r != 0 || !radix_supported(r)) continue;
+            auto sub = best(m / r);
+            if (sub.first >= 1e29) continue;
+            const double c = sub.first + radix_cost(r);
+            if (c < res.first) {
+                res.first = c;
+                res.second = sub.second;
+                res.second.push_back(r);
+            }
+        }
+        memo[m] = res;
+        return res;
+    };
+    auto r = best(n);
+    if (r.first >= 1e29) return {-1};
+    std::sort(r.second.begin(), r.second.end(), std::greater<int>());
+    return r.second;
+}
+
+namespace {
+
+bool factorizable(int n, int e) {
+    if (n == 1) return true;
+    auto r = choose_radices(n, e);
+    return !(r.size() == 1 && r[0] == -1);
+}
+
+PlanDev make_plandev(int n, const std::vector<int>& radices, int* tw_entries) {
+    PlanDev pd{};
+    pd.N = n;
+    pd.npass = (int)radices.size();
+    if (pd.npass > kMaxPasses) throw PlanError(ACL_ERROR_INTERNAL_ERROR, "too many passes");
+    int L = 1, off = 0;
+    for (int i = 0; i < pd.npass; ++i) {
+        PassDesc& p = pd.pass[i];
+        p.R = radices[i];
+        p.L = L;
+        p.tw = off;
+        p.nr = make_fastdiv((uint32_t)(n / p.R));
+        p.l = make_fastdiv((uint32_t)L);
+        if (L > 1) off += L * (p.R - 1);
+        L *= p.R;
+    }
+    *tw_entries = off;
+    return pd;
+}
+
+int even_ld(int rowlen) {
+    int ld = sidx(rowlen - 1) + 1;
+    if ((ld & 1) == 0) ++ld;
+    return ld;
+}
+
+constexpr int kSmemLimit = 227 * 1024;
+constexpr int kRowTileBytes = 64 * 1024;
+
+struct TileShape {
+    int e, P, T, LD, smem;
+};
+
+// `column`: the tile's transforms are adjacent in memory on the load or
+// store side, so P sets the contiguous run length (8-16 values wanted).
+TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
+    TileShape s{};
+    s.e = (n > 8192 || (column && n >= 1024)) ? 32 : 16;
+    s.LD = even_ld(std::max(rowlen, 1));
+    const long long row_bytes = (long long)s.LD * 8;
+    long long maxp_thr = std::max<long long>(1, (long long)kMaxTileThreads * s.e / std::max(n, 1));
+    long long p;
+    if (column) {
+        p = std::min<long long>({16, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
+    } else {
+        p = std::min<long long>(maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes));
+    }
+    p = std::max<long long>(1, std::min<long long>(p, transforms));
+    s.P = (int)p;
+    long long t = ((long long)s.P * n + s.e - 1) / s.e;
+    t = std::max<long long>(32, (t + 31) / 32 * 32);
+    s.T = (int)std::min<long long>(t, kMaxTileThreads);
+    s.smem = (int)(s.P * row_bytes);
+    if (s.smem > kSmemLimit) throw PlanError(ACL_ERROR_INTERNAL_ERROR, "tile does not fit shared memory");
+    return s;
+}
+
+struct AxisIO {
+    long long inner = 1, outer = 1;
+    long long in_odist = 0, in_idist = 0, in_stride = 1;
+    long long out_odist = 0, out_idist = 0, out_stride = 1;
+};
+
+// One tile launch.  n = FFT length of each tile transform; rowlen = values
+// a shared-memory row must hold; transforms = inner * outer.
+Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const AxisIO& io, int flags, int rows,
+                    const std::string& what) {
+    Step st;
+    const long long transforms = io.inner;
+    TileShape sh = pick_shape(n, rowlen, column, transforms);
+    st.radices = choose_radices(n, sh.e);
+    if (st.radices.size() == 1 && st.radices[0] == -1)
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " has no supported radix plan");
+    int tw_entries = 0;
+    st.host_plan = make_plandev(n, st.radices, &tw_entries);
+    TileLaunch& L = st.L;
+    L.sign = sign;
+    L.e = sh.e;
+    L.op = op;
+    L.block = sh.T;
+    L.smem_bytes = sh.smem;
+    TileArgs& a = L.args;
+    a.N = n;
+    a.P = sh.P;
+    a.LD = sh.LD;
+    a.inner = (int)io.inner;
+    a.tiles_per_outer = (int)((io.inner + sh.P - 1) / sh.P);
+    const long long ntiles = (long long)a.tiles_per_outer * io.outer;
+    if (ntiles > 0x7fffffffLL || io.inner > 0x7fffffffLL)
+        throw PlanError(ACL_ERROR_INVALID_PARAM, "too many transforms");
+    a.ntiles = (int)ntiles;
+    a.in_odist = io.in_odist;
+    a.in_idist = io.in_idist;
+    a.in_stride = io.in_stride;
+    a.out_odist = io.out_odist;
+    a.out_idist = io.out_idist;
+    a.out_stride = io.out_stride;
+    a.rows = rows;
+    a.flags = flags;
+    a.scale = 1.0f;
+    a.div_n = make_fastdiv((uint32_t)std::max(n, 1));
+    a.div_p = make_fastdiv((uint32_t)sh.P);
+    const int h = (op == OP_R2C_HALF || op == OP_C2R_HALF) ? n + 1 : n / 2 + 1;
+    a.div_h = make_fastdiv((uint32_t)h);
+    a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+    L.grid = a.ntiles;
+    st.what = what;
+    (void)tw_entries;
+    return st;
+}
+
+int c2c_sign(const FftPlan& plan) { return plan.forward() ? -1 : 1; }
+
+// Splits n > kMaxTileN into n1 (column pass) * n2 (row pass), both one
+// tile long and factorizable, n1 <= n2 and as balanced as possible.
+bool four_step_split(long long n, int* n1, int* n2) {
+    int best1 = 0;
+    for (long long a = 2; a * a <= n; ++a) {
+        if (n % a) continue;
+        const long long b = n / a;
+        if (b > kMaxTileN || a > kMaxTileN) continue;
+        if (!factorizable((int)a, 32) || !factorizable((int)b, 32)) continue;
+        best1 = (int)a;  // ascending a: the last hit is the most balanced
+    }
+    if (best1 == 0) return false;
+    *n1 = best1;
+    *n2 = (int)(n / best1);
+    return true;
+}
+
+struct C2COpts {
+    int sign = 0;        // 0: the plan's direction
+    int last_flags = 0;  // flags of the final pass (scaling)
+    float last_scale = 1.0f;
+    Loc src = Loc::In, dst = Loc::Out;
+    size_t src_off = 0, dst_off = 0;
+    size_t scratch_off = 0;  // four-step scratch region in the workspace
+};
+
+void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
+    const int sign = o.sign != 0 ? o.sign : c2c_sign(plan);
+    if (n <= kMaxTileN) {
+        AxisIO io;
+        io.inner = batch;
+        io.in_idist = n;
+        io.out_idist = n;
+        Step st = make_tile_step(OP_C2C, sign, (int)n, (int)n, false, io, o.last_flags, 0,
+                                 "c2c rows n=" + std::to_string(n));
+        st.L.args.scale = o.last_scale;
+        st.src = o.src;
+        st.dst = o.dst;
+        st.src_off = o.src_off;
+        st.dst_off = o.dst_off;
+        plan.steps.push_back(st);
+        return;
+    }
+    int n1 = 0, n2 = 0;
+    if (!four_step_split(n, &n1, &n2))
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " has no four-step split");
+    // Pass A: n1-point FFTs down the n2 columns of x viewed as [n1][n2],
+    // times W_n^{n2 k1}, into the workspace as Y[k1][n2]
+    // (reference: phase A of core/fft/fftcore/fft_c2c_large.cpp:199-204).
+    AxisIO a;
+    a.inner = n2;
+    a.outer = batch;
+    a.in_odist = n;
+    a.in_idist = 1;
+    a.in_stride = n2;
+    a.out_odist = n;
+    a.out_idist = 1;
+    a.out_stride = n2;
+    Step sa = make_tile_step(OP_C2C, sign, n1, n1, true, a, 0, 0,
+                             "four-step A n=" + std::to_string(n) + " n1=" + std::to_string(n1));
+    sa.L.tw4 = true;
+    sa.tw2_kind = 1;
+    sa.tw2_n = n;
+    sa.tw2_count = n;
+    sa.src = o.src;
+    sa.src_off = o.src_off;
+    sa.dst = Loc::Ws;
+    sa.dst_off = o.scratch_off;
+    // Pass B: n2-point FFTs along the rows of Y; X[k1 + n1 k2] is stored
+    // with stride n1, so adjacent rows of a tile are adjacent outputs.
+    AxisIO b;
+    b.inner = n1;
+    b.outer = batch;
+    b.in_odist = n;
+    b.in_idist = n2;
+    b.in_stride = 1;
+    b.out_odist = n;
+    b.out_idist = 1;
+    b.out_stride = n1;
+    Step sb = make_tile_step(OP_C2C, sign, n2, n2, true, b, o.last_flags, 0,
+                             "four-step B n=" + std::to_string(n) + " n2=" + std::to_string(n2));
+    sb.L.args.scale = o.last_scale;
+    sb.src = Loc::Ws;
+    sb.src_off = o.scratch_off;
+    sb.dst = o.dst;
+    sb.dst_off = o.dst_off;
+    plan.steps.push_back(sa);
+    plan.steps.push_back(sb);
+    plan.workspace_need = std::max(plan.workspace_need, o.scratch_off + (size_t)(batch * n * 8));
+}
+
+// Real transform along contiguous rows of length n (rows rows), one tile.
+void add_real_rows(FftPlan& plan, bool r2c, long long n, long long rows, Loc src, Loc dst) {
+    const long long h = n / 2 + 1;
+    const int flags = r2c ? (plan.forward() ? 0 : TF_CONJ_OUT) : (plan.forward() ? TF_CONJ_IN : 0);
+    if (n % 2 == 0) {
+        const int m = (int)(n / 2);
+        AxisIO io;
+        io.inner = rows;
+        io.in_idist = r2c ? m : h;
+        io.out_idist = r2c ? h : m;
+        Step st = make_tile_step(r2c ? OP_R2C_HALF : OP_C2R_HALF, r2c ? -1 : 1, m, r2c ? m : m + 1, false, io, flags,
+                                 (int)rows, std::string(r2c ? "r2c" : "c2r") + " half n=" + std::to_string(n));
+        st.tw2_kind = 1;
+        st.tw2_n = n;
+        st.tw2_count = m + 1;
+        st.src = src;
+        st.dst = dst;
+        plan.steps.push_back(st);
+        return;
+    }
+    AxisIO io;
+    io.inner = (rows + 1) / 2;
+    io.in_idist = r2c ? n : h;
+    io.out_idist = r2c ? h : n;
+    Step st = make_tile_step(r2c ? OP_R2C_PAIR : OP_C2R_PAIR, r2c ? -1 : 1, (int)n, (int)n, false, io, flags,
+                             (int)rows, std::string(r2c ? "r2c" : "c2r") + " pair n=" + std::to_string(n));
+    st.src = src;
+    st.dst = dst;
+    plan.steps.push_back(st);
+}
+
+bool real_fits_tile(long long n) { return (n % 2 == 0) ? n / 2 <= kMaxTileN : n <= kMaxTileN; }
+
+// Even real length whose half-length FFT needs the four-step split: the
+// complex four-step over the workspace plus an element-wise pre/post pass.
+// Workspace: [0, zbytes) four-step scratch, [zoff, zoff + zbytes) Z.
+void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
+    if (n % 2 != 0)
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "odd real length " + std::to_string(n) + " above one tile");
+    const long long m = n / 2;
+    const size_t zbytes = (size_t)(rows * m * 8);
+    const size_t zoff = (zbytes + 255) / 256 * 256;
+    Step pp;
+    pp.kind = r2c ? StepKind::RealPost : StepKind::RealPre;
+    pp.real.m = m;
+    pp.real.rows = rows;
+    pp.real.conj = r2c ? (plan.forward() ? 0 : 1) : (plan.forward() ? 1 : 0);
+    pp.tw2_kind = 1;
+    pp.tw2_n = n;
+    pp.tw2_count = m + 1;
+    C2COpts o;
+    o.scratch_off = 0;
+    if (r2c) {
+        pp.real.in_pitch = m;
+        pp.real.out_pitch = m + 1;
+        pp.src = Loc::Ws;
+        pp.src_off = zoff;
+        pp.dst = Loc::Out;
+        pp.what = "r2c post n=" + std::to_string(n);
+        o.sign = -1;
+        o.src = Loc::In;
+        o.dst = Loc::Ws;
+        o.dst_off = zoff;
+        add_c2c_1d(plan, m, rows, o);
+        plan.steps.push_back(pp);
+    } else {
+        pp.real.in_pitch = m + 1;
+        pp.real.out_pitch = m;
+        pp.src = Loc::In;
+        pp.dst = Loc::Ws;
+        pp.dst_off = zoff;
+        pp.what = "c2r pre n=" + std::to_string(n);
+        plan.steps.push_back(pp);
+        o.sign = 1;
+        o.src = Loc::Ws;
+        o.src_off = zoff;
+        o.dst = Loc::Out;
+        o.last_flags = TF_SCALE;
+        o.last_scale = 2.0f;
+        add_c2c_1d(plan, m, rows, o);
+    }
+    plan.workspace_need = std::max(plan.workspace_need, zoff + zbytes);
+}
+
+}  // namespace
+
+void build_steps(FftPlan& plan) {
+    plan.steps.clear();
+    plan.workspace_need = 0;
+    const long long b = plan.batch;
+    const auto& sz = plan.sizes;
+    const bool c2c = plan.type == ASCEND_FFT_C2C || plan.type == ASCEND_FFT_C2C_SEP;
+    const bool r2c = plan.type == ASCEND_FFT_R2C;
+    if (sz.size() == 1) {
+        const long long n = sz[0];
+        if (c2c) {
+            add_c2c_1d(plan, n, b, C2COpts{});
+        } else if (real_fits_tile(n)) {
+            add_real_rows(plan, r2c, n, b, Loc::In, Loc::Out);
+        } else {
+            add_real_large(plan, r2c, n, b);
+        }
+        return;
+    }
+    // Multi-dimensional: the last axis is contiguous, the others are
+    // strided column passes done in place on the destination.
+    const int nd = (int)sz.size();
+    for (int i = 0; i < nd - 1; ++i)
+        if (sz[i] > kMaxTileN)
+            throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
+    const long long last = sz[nd - 1];
+    if (c2c ? last > kMaxTileN : !real_fits_tile(last))
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
+    const long long lastc = c2c ? last : last / 2 + 1;  // complex extent of the last axis
+    long long rows = b;
+    for (int i = 0; i < nd - 1; ++i) rows *= sz[i];
+    // Column pass along axis `ax` of the complex array [b][sz0]..[lastc].
+    auto column_pass = [&](int ax, Loc src, Loc dst) {
+        long long inner = lastc;
+        for (int i = ax + 1; i < nd - 1; ++i) inner *= sz[i];
+        long long outer = b;
+        for (int i = 0; i < ax; ++i) outer *= sz[i];
+        const long long n = sz[ax];
+        AxisIO io;
+        io.inner = inner;
+        io.outer = outer;
+        io.in_odist = n * inner;
+        io.in_idist = 1;
+        io.in_stride = inner;
+        io.out_odist = n * inner;
+        io.out_idist = 1;
+        io.out_stride = inner;
+        Step st = make_tile_step(OP_C2C, c2c_sign(plan), (int)n, (int)n, true, io, 0, 0,
+                                 "c2c axis " + std::to_string(ax) + " n=" + std::to_string(n));
+        st.src = src;
+        st.dst = dst;
+        plan.steps.push_back(st);
+    };
+    if (c2c) {
+        AxisIO io;
+        io.inner = rows;
+        io.in_idist = last;
+        io.out_idist = last;
+        Step st = make_tile_step(OP_C2C, c2c_sign(plan), (int)last, (int)last, false, io, 0, 0,
+                                 "c2c axis " + std::to_string(nd - 1) + " n=" + std::to_string(last));
+        st.src = Loc::In;
+        st.dst = Loc::Out;
+        plan.steps.push_back(st);
+        for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
+    } else if (r2c) {
+        add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
+        for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
+    } else {
+        column_pass(nd - 2, Loc::In, Loc::Ws);
+        for (int ax = nd - 3; ax >= 0; --ax) column_pass(ax, Loc::Ws, Loc::Ws);
+        add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
+        plan.workspace_need = (size_t)(rows * lastc * 8);
+    }
+}
+
+std::string describe(const FftPlan& plan) {
+    static const char* locs[] = {"in", "out", "ws"};
+    std::ostringstream os;
+    os << "{\"type\":" << (int)plan.type << ",\"forward\":" << (plan.forward() ? "true" : "false")
+       << ",\"batch\":" << plan.batch << ",\"sizes\":[";
+    for (size_t i = 0; i < plan.sizes.size(); ++i) os << (i ? "," : "") << plan.sizes[i];
+    os << "],\"workspace\":" << plan.workspace_need << ",\"steps\":[";
+    for (size_t i = 0; i < plan.steps.size(); ++i) {
+        const Step& st = plan.steps[i];
+        os << (i ? "," : "") << "{\"what\":\"" << st.what << "\",\"kind\":" << (int)st.kind << ",\"src\":\""
+           << locs[(int)st.src] << "\",\"dst\":\"" << locs[(int)st.dst] << "\",\"src_off\":" << st.src_off
+           << ",\"dst_off\":" << st.dst_off;
+        if (st.kind == StepKind::Tile) {
+            const TileArgs& a = st.L.args;
+            os << ",\"op\":" << st.L.op << ",\"sign\":" << st.L.sign << ",\"e\":" << st.L.e << ",\"n\":" << a.N
+               << ",\"P\":" << a.P << ",\"LD\":" << a.LD << ",\"threads\":" << st.L.block << ",\"grid\":" << st.L.grid
+               << ",\"smem\":" << st.L.smem_bytes << ",\"tw4\":" << (st.L.tw4 ? "true" : "false")
+               << ",\"flags\":" << a.flags << ",\"inner\":" << a.inner << ",\"tiles_per_outer\":" << a.tiles_per_outer
+               << ",\"in\":[" << a.in_odist << "," << a.in_idist << "," << a.in_stride << "],\"out\":["
+               << a.out_odist << "," << a.out_idist << "," << a.out_stride << "],\"radices\":[";
+            for (size_t r = 0; r < st.radices.size(); ++r) os << (r ? "," : "") << st.radices[r];
+            os << "]";
+        } else {
+            os << ",\"m\":" << st.real.m << ",\"rows\":" << st.real.rows << ",\"conj\":" << st.real.conj;
+        }
+        os << "}";
+    }
+    os << "]}";
+    return os.str();
+}
+
+}  // namespace sipfft

@@ -1,0 +1,97 @@
+// Plan model of the B200 FFT library: a plan is an ordered list of tile
+// kernel launches ("steps") whose operands are the exec's input, output or
+// a region of the caller's workspace.  It replaces the reference's
+// FFTPlan{steps[]} of FftOperation cores (core/fft/fftplan/include/fftplan/
+// fft_plan.h:43-71) with direct CUDA launches.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fft_api.h"
+#include "real_kernels.h"
+#include "tile_launch.h"
+
+namespace sipfft {
+
+// Error carrying the status code the C ABI returns.
+struct PlanError : std::runtime_error {
+    int code;
+    PlanError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Device allocation owned by plans through shared_ptr (tables are shared
+// between plans through TableCache).
+struct DeviceBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    ~DeviceBuf();
+};
+using BufPtr = std::shared_ptr<DeviceBuf>;
+
+// Operand of a step.
+enum class Loc : int { In = 0, Out = 1, Ws = 2 };
+
+enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2 };
+
+struct Step {
+    StepKind kind = StepKind::Tile;
+    TileLaunch L;
+    RealPassArgs real{};  // RealPost / RealPre
+    Loc src = Loc::In, dst = Loc::Out;
+    size_t src_off = 0, dst_off = 0;  // byte offsets into the operand
+    PlanDev host_plan{};              // pass list (uploaded to plan_dev)
+    std::vector<int> radices;
+    int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count
+    long long tw2_n = 0, tw2_count = 0;
+    BufPtr plan_dev, tw, tw2;
+    std::string what;                 // human-readable description
+};
+
+struct FftPlan {
+    AsdSip::asdFftType type = AsdSip::ASCEND_FFT_C2C;
+    AsdSip::asdFftDirection direction = AsdSip::ASCEND_FFT_FORWARD;
+    std::vector<int64_t> sizes;  // transform dims, outermost first
+    int64_t batch = 1;
+    bool vertical = false;
+    bool initialized = false;
+    bool resources_ready = false;
+    int device = -1;
+    void* stream = nullptr;
+    void* workspace = nullptr;
+    size_t workspace_recorded = 0;  // value recorded by GetWorkspaceSize
+    size_t workspace_need = 0;
+    std::vector<Step> steps;
+
+    bool forward() const { return direction == AsdSip::ASCEND_FFT_FORWARD; }
+    int64_t elements() const;  // batch * prod(sizes)
+};
+
+// Radix sequence for a length that fits one tile; empty if the length has
+// a prime factor without a compiled butterfly.
+std::vector<int> choose_radices(int n, int e);
+
+// Largest complex length one tile kernel transforms (shared memory bound).
+constexpr int kMaxTileN = 16384;
+
+// Builds the steps of a validated plan (host side only).
+void build_steps(FftPlan& plan);
+
+// Allocates the plan's device tables on the current device.
+void prepare_device(FftPlan& plan);
+
+// Launches every step on the plan's stream.
+void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws);
+
+// JSON description of the steps (tests, ASDSIP_FFT_PLAN_TRACE).
+std::string describe(const FftPlan& plan);
+
+}  // namespace sipfft

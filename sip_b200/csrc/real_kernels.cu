@@ -1,0 +1,50 @@
+// Real-transform pre/post passes for lengths beyond one tile (element
+// formulas in real_math.cuh).
+#include "real_kernels.h"
+
+#include "real_math.cuh"
+
+namespace sipfft {
+
+namespace {
+
+__global__ void k_real_post(const RealPassArgs a) {
+    for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
+        const float2* z = a.src + row * a.in_pitch;
+        float2* x = a.dst + row * a.out_pitch;
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k <= a.m;
+             k += (long long)gridDim.x * blockDim.x)
+            x[k] = real_post_elem(z, k, a.m, a.tw, a.conj != 0);
+    }
+}
+
+__global__ void k_real_pre(const RealPassArgs a) {
+    for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
+        const float2* x = a.src + row * a.in_pitch;
+        float2* z = a.dst + row * a.out_pitch;
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < a.m;
+             k += (long long)gridDim.x * blockDim.x)
+            z[k] = real_pre_elem(x, k, a.m, a.tw, a.conj != 0);
+    }
+}
+
+dim3 grid_for(long long per_row, long long rows, int block) {
+    long long gx = (per_row + block - 1) / block;
+    if (gx > 4096) gx = 4096;
+    long long gy = rows < 65535 ? rows : 65535;
+    return dim3((unsigned)gx, (unsigned)gy, 1);
+}
+
+}  // namespace
+
+cudaError_t real_post(const RealPassArgs& a, cudaStream_t stream) {
+    k_real_post<<<grid_for(a.m + 1, a.rows, 256), 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t real_pre(const RealPassArgs& a, cudaStream_t stream) {
+    k_real_pre<<<grid_for(a.m, a.rows, 256), 256, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace sipfft

@@ -1,0 +1,42 @@
+// Element formulas of the real-transform pre/post passes for lengths
+// beyond one tile, shared by real_kernels.cu and the CPU test harness.
+// They are the formulas of the fused tile stores/loads in tile_io.cuh,
+// after the reference's fft_real_stockham_r2c.cpp:60-105 (post-process)
+// and fft_real_stockham_c2r.cpp:73-100 (even pre-process).
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace sipfft {
+
+// X[k], k in [0, m], from the half-length spectrum row z (m values).
+SIP_HD float2 real_post_elem(const float2* z, long long k, long long m, const float2* tw, bool conj) {
+    const float2 zk = SIP_LDG(z + (k == m ? 0 : k));
+    const float2 zm = SIP_LDG(z + (k == 0 ? 0 : m - k));
+    const float2 b = make_float2(zm.x, -zm.y);
+    const float2 ev = make_float2(0.5f * (zk.x + b.x), 0.5f * (zk.y + b.y));
+    const float2 od = make_float2(0.5f * (zk.y - b.y), -0.5f * (zk.x - b.x));
+    float2 v = c_add(ev, c_mul(SIP_LDG(tw + k), od));
+    if (conj) v.y = -v.y;
+    return v;
+}
+
+// Z[k], k in [0, m), from the half spectrum row x (m + 1 values).
+SIP_HD float2 real_pre_elem(const float2* x, long long k, long long m, const float2* tw, bool conj) {
+    if (k == 0) {
+        const float dc = SIP_LDG(x).x, ny = SIP_LDG(x + m).x;
+        return make_float2(0.5f * (dc + ny), 0.5f * (dc - ny));
+    }
+    float2 xv = SIP_LDG(x + k), yv = SIP_LDG(x + m - k);
+    if (conj) {
+        xv.y = -xv.y;
+        yv.y = -yv.y;
+    }
+    const float2 b = make_float2(yv.x, -yv.y);
+    const float2 e = make_float2(0.5f * (xv.x + b.x), 0.5f * (xv.y + b.y));
+    const float2 d = make_float2(0.5f * (xv.x - b.x), 0.5f * (xv.y - b.y));
+    const float2 od = c_mulc(d, SIP_LDG(tw + k));
+    return make_float2(e.x - od.y, e.y + od.x);
+}
+
+}  // namespace sipfft

@@ -1,0 +1,51 @@
+// Host-side dispatch of the tile kernels compiled in tile_inst.cu.
+#include <cuda_runtime.h>
+
+#include "tile_launch.h"
+
+namespace sipfft {
+
+using KernelFn = void (*)(const TileArgs);
+
+KernelFn tile_pick_fwd_e16(int op, bool tw4);
+KernelFn tile_pick_fwd_e32(int op, bool tw4);
+KernelFn tile_pick_inv_e16(int op, bool tw4);
+KernelFn tile_pick_inv_e32(int op, bool tw4);
+
+namespace {
+
+KernelFn pick_kernel(int sign, int e, int op, bool tw4) {
+    if (sign < 0) {
+        if (e == 16) return tile_pick_fwd_e16(op, tw4);
+        if (e == 32) return tile_pick_fwd_e32(op, tw4);
+    } else {
+        if (e == 16) return tile_pick_inv_e16(op, tw4);
+        if (e == 32) return tile_pick_inv_e32(op, tw4);
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes) {
+    KernelFn fn = pick_kernel(sign, e, op, tw4);
+    if (fn == nullptr) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_bytes);
+}
+
+cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream) {
+    KernelFn fn = pick_kernel(L.sign, L.e, L.op, L.tw4);
+    if (fn == nullptr) return cudaErrorInvalidValue;
+    TileArgs a = L.args;
+    a.src = src;
+    a.dst = dst;
+    fn<<<L.grid, L.block, L.smem_bytes, stream>>>(a);
+    return cudaGetLastError();
+}
+
+const void* tile_kernel_address(int sign, int e, int op, bool tw4) {
+    return reinterpret_cast<const void*>(pick_kernel(sign, e, op, tw4));
+}
+
+}  // namespace sipfft

@@ -1,0 +1,41 @@
+// Host-side description of one tile-kernel launch and the entry points of
+// tile_kernels.cu / twiddle.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft_core.cuh"
+#include "tile_io.cuh"
+
+namespace sipfft {
+
+constexpr int kMaxTileThreads = 512;
+
+struct TileLaunch {
+    int sign = -1;  // -1 forward, +1 inverse
+    int e = 16;     // elements per thread (compiled variants: 16, 32)
+    int op = OP_C2C;
+    bool tw4 = false;
+    int grid = 0;
+    int block = 0;
+    int smem_bytes = 0;
+    TileArgs args{};  // src / dst are bound per exec
+};
+
+// Sets the dynamic shared-memory limit of the selected instantiation.
+cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes);
+
+cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream);
+
+const void* tile_kernel_address(int sign, int e, int op, bool tw4);
+
+// Twiddle tables, generated on the device in FP64 (sincospi) and rounded
+// once to FP32.  All tables hold forward values exp(-2 pi i m / n).
+
+// Stockham table for the pass list of `plan` (entries plan.N - 1 at most).
+cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries, cudaStream_t stream);
+
+// out[k] = exp(-2 pi i k / n), k in [0, count).
+cudaError_t gen_root_twiddles(float2* out, long long n, long long count, cudaStream_t stream);
+
+}  // namespace sipfft

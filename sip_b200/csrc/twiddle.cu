@@ -1,0 +1,65 @@
+// Twiddle-table generation on the device.
+//
+// Angles are formed from exact integers (m, n) and evaluated with FP64
+// sincospi, then rounded once to FP32, following the reference's
+// FP64-then-round coefficient builders
+// (ops/include/params/fft_real_stockham.h:77-111,
+// ops/fft/c2c/fft_regbase/fft_regbase/large/fft_c2c_coefficients.h:17-90).
+#include <cuda_runtime.h>
+
+#include "tile_launch.h"
+
+namespace sipfft {
+
+namespace {
+
+__device__ __forceinline__ float2 root_fwd(long long m, long long n) {
+    m %= n;
+    if (m < 0) m += n;
+    double s, c;
+    sincospi(2.0 * (double)m / (double)n, &s, &c);
+    return make_float2((float)c, (float)(-s));
+}
+
+__global__ void k_stockham_tw(float2* out, const PlanDev plan, int entries) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= entries) return;
+    for (int p = 0; p < plan.npass; ++p) {
+        const PassDesc& pd = plan.pass[p];
+        if (pd.L <= 1) continue;
+        const int cnt = pd.L * (pd.R - 1);
+        if (i >= pd.tw && i < pd.tw + cnt) {
+            const int off = i - pd.tw;
+            const int k = off / (pd.R - 1);
+            const int r = off - k * (pd.R - 1) + 1;
+            out[i] = root_fwd((long long)r * k, (long long)pd.L * pd.R);
+            return;
+        }
+    }
+}
+
+__global__ void k_root_tw(float2* out, long long n, long long count) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = root_fwd(i, n);
+}
+
+}  // namespace
+
+cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries, cudaStream_t stream) {
+    if (entries <= 0) return cudaSuccess;
+    const int block = 256;
+    k_stockham_tw<<<(entries + block - 1) / block, block, 0, stream>>>(out, plan, entries);
+    return cudaGetLastError();
+}
+
+cudaError_t gen_root_twiddles(float2* out, long long n, long long count, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    const int block = 256;
+    long long blocks = (count + block - 1) / block;
+    if (blocks > 65535LL * 16) blocks = 65535LL * 16;
+    k_root_tw<<<(unsigned)blocks, block, 0, stream>>>(out, n, count);
+    return cudaGetLastError();
+}
+
+}  // namespace sipfft

@@ -1,0 +1,33 @@
+"""Builds the CPU harness tests/native/libtile_emu.so (test infrastructure).
+
+The harness links the library's planner (sip_b200/csrc/plan.cpp) with
+tests/native/tile_emu.cpp, which drives the kernels' host-device phase
+functions on the CPU.
+"""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+CSRC = ROOT / "sip_b200" / "csrc"
+LIB = HERE / "libtile_emu.so"
+NVCC = "/usr/local/cuda/bin/nvcc"
+
+
+def build() -> Path:
+    srcs = [HERE / "tile_emu.cpp", CSRC / "plan.cpp"]
+    deps = srcs + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").rglob("*.h"))
+    if LIB.exists() and LIB.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return LIB
+    cmd = [NVCC, "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared", "-I", str(ROOT / "include"),
+           "-I", str(CSRC), *map(str, srcs), "-o", str(LIB)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"harness build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build())

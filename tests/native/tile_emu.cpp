@@ -1,0 +1,223 @@
+// CPU harness for the FFT kernels (test infrastructure only).
+//
+// Builds a plan with the library's own planner (sip_b200/csrc/plan.cpp)
+// and runs every step on the host by calling the kernels' own
+// __host__ __device__ phase functions (tile_io.cuh loads/stores,
+// fft_core.cuh pass_read / pass_write, real_math.cuh) for every thread
+// index of every tile, with a barrier between phases emulated by running
+// each phase for all threads before the next.  This checks the planner,
+// the index arithmetic and the butterflies against numpy without a GPU.
+// Shared memory is filled with NaN before each tile so a read of a slot no
+// phase wrote shows up in the result.  Twiddles are computed on the host
+// in long double and rounded once to float.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+#include "real_math.cuh"
+
+using namespace sipfft;
+
+namespace {
+
+float2 root_host(long long m, long long n) {
+    m %= n;
+    if (m < 0) m += n;
+    const long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+    return make_float2((float)std::cos(a), (float)(-std::sin(a)));
+}
+
+std::vector<float2> stockham_host(const PlanDev& pd) {
+    int entries = 0;
+    for (int i = 0; i < pd.npass; ++i)
+        if (pd.pass[i].L > 1) entries = pd.pass[i].tw + pd.pass[i].L * (pd.pass[i].R - 1);
+    std::vector<float2> t(std::max(entries, 1));
+    for (int i = 0; i < pd.npass; ++i) {
+        const PassDesc& p = pd.pass[i];
+        if (p.L <= 1) continue;
+        for (int k = 0; k < p.L; ++k)
+            for (int r = 1; r < p.R; ++r) t[p.tw + k * (p.R - 1) + r - 1] = root_host((long long)r * k, (long long)p.L * p.R);
+    }
+    return t;
+}
+
+template <int R, int SIGN, int S>
+void emu_pass(int T, const TileArgs& a, float2* sm, const PassDesc& pd) {
+    std::vector<PassRegs<R, S>> regs(T);
+    for (int tid = 0; tid < T; ++tid) pass_read<R, SIGN, S>(tid, T, a.P, a.N, sm, a.LD, pd, a.tw, regs[tid]);
+    for (int tid = 0; tid < T; ++tid) pass_write<R, S>(tid, T, a.P, sm, a.LD, pd, regs[tid]);
+}
+
+template <int SIGN, int E>
+void emu_passes(int T, const TileArgs& a, float2* sm) {
+    for (int i = 0; i < a.plan->npass; ++i) {
+        const PassDesc& pd = a.plan->pass[i];
+        switch (pd.R) {
+#define SIP_EMU_CASE(R)                               \
+    case R:                                           \
+        emu_pass<R, SIGN, cdiv(E, R)>(T, a, sm, pd);  \
+        break;
+            SIP_FFT_FOR_EACH_RADIX(SIP_EMU_CASE)
+#undef SIP_EMU_CASE
+            default:
+                throw std::runtime_error("radix without a pass");
+        }
+    }
+}
+
+void emu_tile_step(const Step& st, const void* src, void* dst) {
+    TileArgs a = st.L.args;
+    a.src = src;
+    a.dst = dst;
+    a.plan = &st.host_plan;
+    std::vector<float2> tw = stockham_host(st.host_plan);
+    std::vector<float2> tw2;
+    if (st.tw2_kind == 1) {
+        tw2.resize(st.tw2_count);
+        for (long long k = 0; k < st.tw2_count; ++k) tw2[k] = root_host(k, st.tw2_n);
+    }
+    a.tw = tw.data();
+    a.tw2 = tw2.empty() ? nullptr : tw2.data();
+    const int T = st.L.block;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    std::vector<float2> smv((size_t)a.P * a.LD);
+    float2* sm = smv.data();
+    for (int tile = 0; tile < a.ntiles; ++tile) {
+        const TileCtx c = decode_tile(a, tile);
+        for (auto& v : smv) v = make_float2(nan, nan);
+        for (int tid = 0; tid < T; ++tid) {
+            switch (st.L.op) {
+                case OP_C2C: load_c2c(tid, T, a, c, sm); break;
+                case OP_R2C_HALF: load_r2c_half(tid, T, a, c, sm); break;
+                case OP_C2R_HALF: load_c2r_half(tid, T, a, c, sm); break;
+                case OP_R2C_PAIR: load_r2c_pair(tid, T, a, c, sm); break;
+                case OP_C2R_PAIR: load_c2r_pair(tid, T, a, c, sm); break;
+            }
+        }
+        if (st.L.op == OP_C2R_HALF)
+            for (int tid = 0; tid < T; ++tid) prep_c2r_half(tid, T, a, c, sm);
+        if (st.L.sign < 0) {
+            if (st.L.e == 16) emu_passes<-1, 16>(T, a, sm); else emu_passes<-1, 32>(T, a, sm);
+        } else {
+            if (st.L.e == 16) emu_passes<1, 16>(T, a, sm); else emu_passes<1, 32>(T, a, sm);
+        }
+        for (int tid = 0; tid < T; ++tid) {
+            switch (st.L.op) {
+                case OP_C2C:
+                    if (st.L.sign < 0) {
+                        if (st.L.tw4) store_c2c<-1, true>(tid, T, a, c, sm); else store_c2c<-1, false>(tid, T, a, c, sm);
+                    } else {
+                        if (st.L.tw4) store_c2c<1, true>(tid, T, a, c, sm); else store_c2c<1, false>(tid, T, a, c, sm);
+                    }
+                    break;
+                case OP_R2C_HALF: store_r2c_half(tid, T, a, c, sm); break;
+                case OP_C2R_HALF: store_c2r_half(tid, T, a, c, sm); break;
+                case OP_R2C_PAIR: store_r2c_pair(tid, T, a, c, sm); break;
+                case OP_C2R_PAIR: store_c2r_pair(tid, T, a, c, sm); break;
+            }
+        }
+    }
+}
+
+void emu_real_step(const Step& st, const void* src, void* dst) {
+    std::vector<float2> tw(st.tw2_count);
+    for (long long k = 0; k < st.tw2_count; ++k) tw[k] = root_host(k, st.tw2_n);
+    const RealPassArgs& r = st.real;
+    const float2* s = static_cast<const float2*>(src);
+    float2* d = static_cast<float2*>(dst);
+    for (long long row = 0; row < r.rows; ++row) {
+        if (st.kind == StepKind::RealPost) {
+            for (long long k = 0; k <= r.m; ++k)
+                d[row * r.out_pitch + k] = real_post_elem(s + row * r.in_pitch, k, r.m, tw.data(), r.conj != 0);
+        } else {
+            for (long long k = 0; k < r.m; ++k)
+                d[row * r.out_pitch + k] = real_pre_elem(s + row * r.in_pitch, k, r.m, tw.data(), r.conj != 0);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Plans (type, direction, sizes, batch) with the library planner and runs
+// it on host buffers.  Returns 0 on success, the planner's status code on
+// a planning failure, -1 on an emulation failure.  `desc` receives the
+// plan description (JSON) when non-null.
+int emu_exec(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in, void* out,
+             char* desc, size_t desc_cap) {
+    FftPlan p;
+    p.type = static_cast<AsdSip::asdFftType>(type);
+    p.direction = static_cast<AsdSip::asdFftDirection>(direction);
+    p.sizes.assign(sizes, sizes + ndim);
+    p.batch = batch;
+    try {
+        build_steps(p);
+    } catch (const PlanError& e) {
+        if (desc && desc_cap) std::snprintf(desc, desc_cap, "%s", e.what());
+        return e.code;
+    }
+    if (desc && desc_cap) std::snprintf(desc, desc_cap, "%s", describe(p).c_str());
+    try {
+        std::vector<char> ws(p.workspace_need + 16);
+        for (const Step& st : p.steps) {
+            auto resolve = [&](Loc l, size_t off) -> char* {
+                char* base = l == Loc::In ? const_cast<char*>(static_cast<const char*>(in))
+                           : l == Loc::Out ? static_cast<char*>(out) : ws.data();
+                return base + off;
+            };
+            char* s = resolve(st.src, st.src_off);
+            char* d = resolve(st.dst, st.dst_off);
+            if (st.kind == StepKind::Tile) emu_tile_step(st, s, d);
+            else emu_real_step(st, s, d);
+        }
+    } catch (const std::exception&) {
+        return -1;
+    }
+    return 0;
+}
+
+// Fast-division check: returns the number of mismatches of fd_div against
+// exact division over `count` (divisor, dividend) pairs.
+long long emu_fastdiv_check(const unsigned* d, const unsigned* n, long long count) {
+    long long bad = 0;
+    for (long long i = 0; i < count; ++i) {
+        const FastDiv f = make_fastdiv(d[i]);
+        if (fd_div(f, n[i]) != n[i] / d[i]) ++bad;
+    }
+    return bad;
+}
+
+// Radix plan chosen for length n (elements per thread e); writes up to cap
+// radices, returns the count (-1: not factorizable).
+int emu_radices(int n, int e, int* out, int cap) {
+    std::vector<int> r = choose_radices(n, e);
+    if (r.size() == 1 && r[0] == -1) return -1;
+    for (int i = 0; i < (int)r.size() && i < cap; ++i) out[i] = r[i];
+    return (int)r.size();
+}
+
+// One in-register butterfly on host data (checks dft<R, SIGN>).
+int emu_dft(int r, int sign, float* data) {
+    float2* v = reinterpret_cast<float2*>(data);
+    bool ok = true;
+    auto run = [&](auto rc) {
+        constexpr int R = decltype(rc)::value;
+        float2 t[R];
+        for (int i = 0; i < R; ++i) t[i] = v[i];
+        if (sign < 0) dft<R, -1>(t); else dft<R, 1>(t);
+        for (int i = 0; i < R; ++i) v[i] = t[i];
+    };
+    switch (r) {
+#define SIP_EMU_DFT(R) case R: run(std::integral_constant<int, R>{}); break;
+        SIP_FFT_FOR_EACH_RADIX(SIP_EMU_DFT)
+#undef SIP_EMU_DFT
+        default: ok = false;
+    }
+    return ok ? 0 : -1;
+}
+
+}  // extern "C"

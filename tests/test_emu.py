@@ -1,0 +1,89 @@
+"""CPU tests of the kernel arithmetic: the library's planner and the
+kernels' own host-device phase functions, driven on the CPU by
+tests/native/tile_emu.cpp, against the oracle.
+
+Covers every reference unit-test case plus plan kinds the GPU suite runs
+at full size only (four-step, large real, multi-D real, odd batches)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import ref_cases as RC
+from tests.fftcase import emu_run, random_input, shapes
+
+REL_L2_TOL = 1e-6
+
+
+def _check(emu, op, direction, sizes, batch, x=None):
+    if x is None:
+        ishape, idt, _, _ = shapes(op, sizes, batch)
+        x = O.ut_input(ishape, idt)
+    rc, out, desc = emu_run(emu, op, direction, sizes, batch, x)
+    assert rc == 0, desc
+    gold = O.golden(op, direction, x, sizes)
+    err = O.rel_l2(out, O.fp64(op, direction, x, sizes))
+    assert O.ref_check_mismatches(out, gold) == 0, f"rel_l2={err:.3e} {desc[:300]}"
+    assert err <= REL_L2_TOL, desc[:300]
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.C2C_1D)
+def test_ref_c2c_1d(emu, batch, n, direction):
+    _check(emu, O.C2C, direction, [n], batch)
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.R2C_1D)
+def test_ref_r2c_1d(emu, batch, n, direction):
+    _check(emu, O.R2C, direction, [n], batch)
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.C2R_1D)
+def test_ref_c2r_1d(emu, batch, n, direction):
+    _check(emu, O.C2R, direction, [n], batch)
+
+
+@pytest.mark.parametrize("x,y,batch,direction", RC.C2C_2D)
+def test_ref_c2c_2d(emu, x, y, batch, direction):
+    _check(emu, O.C2C, direction, [x, y], batch)
+
+
+@pytest.mark.parametrize("x,y,z,batch,direction", RC.C2C_3D)
+def test_ref_c2c_3d(emu, x, y, z, batch, direction):
+    _check(emu, O.C2C, direction, [x, y, z], batch)
+
+
+@pytest.mark.parametrize("op", [O.C2C, O.R2C, O.C2R])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+@pytest.mark.parametrize("sizes,batch", [([1], 3), ([2], 5), ([3], 4), ([7], 3), ([1000], 5), ([2187], 3),
+                                         ([6000], 2), ([65536], 1), ([40000], 1), ([8, 8], 3), ([30, 33], 3),
+                                         ([9, 7, 5], 2), ([1, 12], 2), ([5, 1, 4], 1)])
+def test_plan_kinds(emu, op, direction, sizes, batch):
+    x = random_input(op, sizes, batch, seed=sum(sizes) + batch)
+    _check(emu, op, direction, sizes, batch, x)
+
+
+def test_radix_butterflies(emu):
+    rng = np.random.default_rng(3)
+    from sip_b200.build import CSRC
+
+    text = (CSRC / "fft_core.cuh").read_text()
+    line = [l for l in text.splitlines() if l.strip().startswith("X(2)")][0]
+    radices = [int(t.strip("X()")) for t in line.split()]
+    assert radices
+    for r in radices:
+        for sign in (-1, 1):
+            x = (rng.standard_normal(r) + 1j * rng.standard_normal(r)).astype(np.complex64)
+            y = x.copy()
+            assert emu.emu_dft(r, sign, y.ctypes.data) == 0
+            ref = np.fft.fft(x.astype(np.complex128)) if sign < 0 else np.fft.ifft(x.astype(np.complex128)) * r
+            assert O.rel_l2(y, ref) < 2e-7, r
+
+
+def test_fastdiv_exact(emu):
+    rng = np.random.default_rng(5)
+    d = np.concatenate([np.arange(1, 5000, dtype=np.uint32), rng.integers(1, 2**31 - 1, 20000).astype(np.uint32)])
+    n = np.concatenate([rng.integers(0, 2**32 - 1, d.size).astype(np.uint32)])
+    edge_d = np.repeat(np.array([1, 2, 3, 7, 641, 65537, 2**31 - 1], np.uint32), 6)
+    edge_n = np.tile(np.array([0, 1, 2**31 - 1, 2**31, 2**32 - 2, 2**32 - 1], np.uint32), 7)
+    d = np.ascontiguousarray(np.concatenate([d, edge_d]))
+    n = np.ascontiguousarray(np.concatenate([n, edge_n]))
+    assert emu.emu_fastdiv_check(d.ctypes.data, n.ctypes.data, d.size) == 0

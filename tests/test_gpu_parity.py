@@ -1,0 +1,79 @@
+"""Parity of the CUDA path with the oracle on a B200, through the C ABI.
+
+Every reference unit-test case (tests/ref_cases.py) runs with the
+reference's own inputs (fixed-seed LCG) and passes the reference's check:
+numpy.fft golden in complex64 / float32, isclose(rtol=1e-3, atol=1e-5)
+(absolute tolerance floored at 1e-6 of the peak, oracle.ref_check_mismatches).
+Each case is also held to rel-L2 <= 1e-6 against the FP64 oracle, the
+accuracy bar of this library.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import ref_cases as RC
+from tests.fftcase import gpu_run, shapes
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_TOL = 1e-6
+
+
+def _check(torch, op, direction, sizes, batch):
+    ishape, idt, _, _ = shapes(op, sizes, batch)
+    x = O.ut_input(ishape, idt)
+    out = gpu_run(torch, op, direction, sizes, batch, x)
+    gold = O.golden(op, direction, x, sizes)
+    bad = O.ref_check_mismatches(out, gold)
+    err = O.rel_l2(out, O.fp64(op, direction, x, sizes))
+    assert bad == 0, f"{bad} elements outside isclose(1e-3, 1e-5); rel_l2={err:.3e}"
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.C2C_1D)
+def test_ref_c2c_1d(cuda, batch, n, direction):
+    _check(cuda, O.C2C, direction, [n], batch)
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.R2C_1D)
+def test_ref_r2c_1d(cuda, batch, n, direction):
+    _check(cuda, O.R2C, direction, [n], batch)
+
+
+@pytest.mark.parametrize("batch,n,direction", RC.C2R_1D)
+def test_ref_c2r_1d(cuda, batch, n, direction):
+    _check(cuda, O.C2R, direction, [n], batch)
+
+
+@pytest.mark.parametrize("x,y,batch,direction", RC.C2C_2D)
+def test_ref_c2c_2d(cuda, x, y, batch, direction):
+    _check(cuda, O.C2C, direction, [x, y], batch)
+
+
+@pytest.mark.parametrize("x,y,z,batch,direction", RC.C2C_3D)
+def test_ref_c2c_3d(cuda, x, y, z, batch, direction):
+    _check(cuda, O.C2C, direction, [x, y, z], batch)
+
+
+# Real multi-dimensional transforms (R2C/C2R along the last axis, C2C on the others).
+@pytest.mark.parametrize("op", [O.R2C, O.C2R])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+@pytest.mark.parametrize("sizes,batch", [([64, 64], 1), ([32, 48], 2), ([500, 50], 2), ([30, 33], 3),
+                                         ([8, 8, 8], 1), ([16, 12, 10], 2), ([9, 7, 5], 2)])
+def test_real_multid(cuda, op, direction, sizes, batch):
+    _check(cuda, op, direction, sizes, batch)
+
+
+@pytest.mark.parametrize("pattern", ["zero", "constant", "impulse", "nyquist", "random"])
+@pytest.mark.parametrize("op", [O.C2C, O.R2C, O.C2R])
+@pytest.mark.parametrize("n", [64, 1000, 4096])
+def test_known_answers(cuda, pattern, op, n):
+    """Known-answer patterns of tests/standalone/fft1d_optimized/run.py:61-107 (FP64 golden, rel-L2)."""
+    for direction in (O.FORWARD, O.INVERSE):
+        x, g = O.kat_input(pattern, op, n, 4, 1, direction)
+        out = gpu_run(cuda, op, direction, [n], 4, x)
+        assert np.isfinite(out).all()
+        if np.linalg.norm(g) == 0:
+            assert np.abs(out).max() == 0
+        else:
+            assert O.rel_l2(out, g) <= REL_L2_TOL
