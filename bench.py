@@ -193,6 +193,8 @@ def run_ours(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     sizes = SIZES if not args.quick else [(n, max(2, b // 64)) for n, b in SIZES]
+    if args.only:
+        sizes = [(n, args.rows or b) for n, b in sizes if n == args.only]
     stream = torch.cuda.Stream(device=dev)
 
     plans = []
@@ -379,6 +381,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="1/64 of the batch (debugging only)")
+    ap.add_argument("--only", type=int, default=0, help="run one size of the workload (profiling)")
+    ap.add_argument("--rows", type=int, default=0, help="rows for --only (profiling a smaller case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")

@@ -123,7 +123,7 @@ int even_ld(int rowlen) {
     return ld;
 }
 
-constexpr int kSmemLimit = 227 * 1024;
+constexpr int kSmemLimit = kMaxTileSmem;
 constexpr int kRowTileBytes = 64 * 1024;
 
 struct TileShape {

@@ -27,11 +27,15 @@ KernelFn pick_kernel(int sign, int e, int op, bool tw4) {
 
 }  // namespace
 
+// The dynamic shared-memory ceiling is an attribute of the kernel function,
+// shared by every plan that launches it, so it is raised once to the
+// per-block maximum rather than set to one plan's tile size.
 cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes) {
     KernelFn fn = pick_kernel(sign, e, op, tw4);
     if (fn == nullptr) return cudaErrorInvalidValue;
+    if (smem_bytes > kMaxTileSmem) return cudaErrorInvalidValue;
     return cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem_bytes);
+                                kMaxTileSmem);
 }
 
 cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream) {

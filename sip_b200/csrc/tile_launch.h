@@ -10,6 +10,8 @@
 namespace sipfft {
 
 constexpr int kMaxTileThreads = 512;
+// Opt-in shared memory per block on sm_100 (227 KB).
+constexpr int kMaxTileSmem = 227 * 1024;
 
 struct TileLaunch {
     int sign = -1;  // -1 forward, +1 inverse

@@ -63,7 +63,7 @@ def gpu_run(torch, op: int, direction: int, sizes, batch: int, x: np.ndarray, st
     h = FftHandle()
     check(make_plan(h, op, direction, list(sizes), batch), "make plan")
     h.bind_workspace()
-    s = stream or torch.cuda.current_stream()
+    s = stream or torch.cuda.Stream()
     check(h.set_stream(s), "set stream")
     fn = {O.C2C: h.exec_c2c, O.R2C: h.exec_r2c, O.C2R: h.exec_c2r}[op]
     check(fn(xt, yt), "exec")
