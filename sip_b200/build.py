@@ -30,6 +30,8 @@ UNITS = [
     ("tile_inst.cu", ["-DSIP_INST_SIGN=-1", "-DSIP_INST_E=32"], "tile_fwd_e32.o"),
     ("tile_inst.cu", ["-DSIP_INST_SIGN=1", "-DSIP_INST_E=16"], "tile_inv_e16.o"),
     ("tile_inst.cu", ["-DSIP_INST_SIGN=1", "-DSIP_INST_E=32"], "tile_inv_e32.o"),
+    *[("sk_shard.cu", [f"-DSIP_SK_SHARD={i}"], f"sk_shard{i}.o") for i in range(8)],
+    ("sk_registry.cu", [], "sk_registry.o"),
     ("tile_kernels.cu", [], "tile_kernels.o"),
     ("twiddle.cu", [], "twiddle.o"),
     ("real_kernels.cu", [], "real_kernels.o"),

@@ -4,6 +4,7 @@
 // weak_ptr, so plans of the same length share one device copy and the
 // copy is freed with its last plan (the reference's FFTensorCache,
 // core/fft/utils/fftensor_cache.cpp:82-101).
+#include <algorithm>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -97,7 +98,16 @@ void prepare_device(FftPlan& plan) {
         st.L.args.plan = static_cast<const PlanDev*>(st.plan_dev->ptr);
         st.L.args.tw = static_cast<const float2*>(st.tw->ptr);
         st.L.args.tw2 = st.tw2 ? static_cast<const float2*>(st.tw2->ptr) : nullptr;
-        check(tile_prepare(st.L.sign, st.L.e, st.L.op, st.L.tw4, st.L.smem_bytes), "cudaFuncSetAttribute");
+        if (st.sk != nullptr) {
+            int per_sm = 1, sms = 1;
+            check(sk_prepare(st.sk->fn, st.L.smem_bytes, st.L.block, &per_sm), "sk_prepare");
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+            const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
+            st.L.grid = (int)std::min<long long>(st.L.args.ntiles, resident);
+            st.L.sk_fn = st.sk->fn;
+        } else {
+            check(tile_prepare(st.L.sign, st.L.e, st.L.op, st.L.tw4, st.L.smem_bytes), "cudaFuncSetAttribute");
+        }
     }
     plan.device = device;
     plan.resources_ready = true;

@@ -301,7 +301,7 @@ SIP_HD uint32_t fd_div(const FastDiv& f, uint32_t n) {
 // Element n of transform p of a tile lives at p * LD + n + n / 16: one pad
 // slot per 16 complex values spreads the strided writes of the early
 // passes over distinct shared-memory bank pairs.
-SIP_HD int sidx(int n) { return n + (n >> 4); }
+SIP_HD constexpr int sidx(int n) { return n + (n >> 4); }
 
 constexpr int kMaxPasses = 12;
 

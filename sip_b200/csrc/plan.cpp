@@ -19,6 +19,7 @@
 #include <tuple>
 
 #include "real_kernels.h"
+#include "sk_registry.h"
 
 namespace sipfft {
 
@@ -162,8 +163,51 @@ struct AxisIO {
 
 // One tile launch.  n = FFT length of each tile transform; rowlen = values
 // a shared-memory row must hold; transforms = inner * outer.
+// Layout mode of a step for the size-specialized kernels, or -1.
+int sk_mode_of(int op, int n, const AxisIO& io) {
+    long long in_row = n, out_row = n;
+    switch (op) {
+        case OP_R2C_HALF: out_row = n + 1; break;
+        case OP_C2R_HALF: in_row = n + 1; break;
+        case OP_R2C_PAIR: out_row = n / 2 + 1; break;
+        case OP_C2R_PAIR: in_row = n / 2 + 1; break;
+        default: break;
+    }
+    if (io.outer == 1 && io.in_stride == 1 && io.out_stride == 1 && io.in_idist == in_row && io.out_idist == out_row)
+        return SK_ROWS;
+    if (op != OP_C2C) return -1;
+    if (io.in_idist == 1 && io.out_idist == 1) return SK_COLS;
+    if (io.in_stride == 1 && io.in_idist == n && io.in_odist == io.inner * n && io.out_idist == 1) return SK_ROWS_T;
+    return -1;
+}
+
+// Switches a generic tile step to a size-specialized kernel when one is
+// compiled for it (its radix order, tile size and threads then apply).
+void try_specialize(Step& st, const AxisIO& io) {
+    TileLaunch& L = st.L;
+    TileArgs& a = L.args;
+    const int mode = sk_mode_of(L.op, a.N, io);
+    if (mode < 0) return;
+    const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N);
+    if (e == nullptr) return;
+    st.sk = e;
+    st.radices = e->radices;
+    int tw_entries = 0;
+    st.host_plan = make_plandev(a.N, st.radices, &tw_entries);
+    L.block = e->T;
+    L.smem_bytes = e->smem;
+    a.P = e->P;
+    a.LD = e->LD;
+    a.tiles_per_outer = (int)((io.inner + e->P - 1) / e->P);
+    a.ntiles = (int)((long long)a.tiles_per_outer * io.outer);
+    a.div_p = make_fastdiv((uint32_t)e->P);
+    a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+    L.grid = a.ntiles;  // capped to the resident CTAs at device preparation
+    st.what += " [sk P=" + std::to_string(e->P) + "]";
+}
+
 Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const AxisIO& io, int flags, int rows,
-                    const std::string& what) {
+                    const std::string& what, bool tw4 = false) {
     Step st;
     const long long transforms = io.inner;
     TileShape sh = pick_shape(n, rowlen, column, transforms);
@@ -203,8 +247,10 @@ Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const Axis
     a.div_h = make_fastdiv((uint32_t)h);
     a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
     L.grid = a.ntiles;
+    L.tw4 = tw4;
     st.what = what;
     (void)tw_entries;
+    if (!std::getenv("SIP_FFT_GENERIC_ONLY")) try_specialize(st, io);
     return st;
 }
 
@@ -269,8 +315,7 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
     a.out_idist = 1;
     a.out_stride = n2;
     Step sa = make_tile_step(OP_C2C, sign, n1, n1, true, a, 0, 0,
-                             "four-step A n=" + std::to_string(n) + " n1=" + std::to_string(n1));
-    sa.L.tw4 = true;
+                             "four-step A n=" + std::to_string(n) + " n1=" + std::to_string(n1), true);
     sa.tw2_kind = 1;
     sa.tw2_n = n;
     sa.tw2_count = n;
@@ -480,7 +525,8 @@ std::string describe(const FftPlan& plan) {
                << ",\"smem\":" << st.L.smem_bytes << ",\"tw4\":" << (st.L.tw4 ? "true" : "false")
                << ",\"flags\":" << a.flags << ",\"inner\":" << a.inner << ",\"tiles_per_outer\":" << a.tiles_per_outer
                << ",\"in\":[" << a.in_odist << "," << a.in_idist << "," << a.in_stride << "],\"out\":["
-               << a.out_odist << "," << a.out_idist << "," << a.out_stride << "],\"radices\":[";
+               << a.out_odist << "," << a.out_idist << "," << a.out_stride << "],\"sk\":" << (st.sk ? "true" : "false")
+               << ",\"radices\":[";
             for (size_t r = 0; r < st.radices.size(); ++r) os << (r ? "," : "") << st.radices[r];
             os << "]";
         } else {

@@ -17,6 +17,7 @@
 
 #include "fft_api.h"
 #include "real_kernels.h"
+#include "sk_registry.h"
 #include "tile_launch.h"
 
 namespace sipfft {
@@ -52,6 +53,7 @@ struct Step {
     std::vector<int> radices;
     int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count
     long long tw2_n = 0, tw2_count = 0;
+    const SkEntry* sk = nullptr;      // size-specialized kernel, when compiled for this step
     BufPtr plan_dev, tw, tw2;
     std::string what;                 // human-readable description
 };

@@ -1,0 +1,385 @@
+// Size-specialized tile FFT kernels ("sk").
+//
+// Same algorithm as the generic tile kernel (fft_core.cuh passes,
+// tile_io.cuh operand layouts) with every size known at compile time:
+// transform length N, radix sequence, transforms per tile P, threads T,
+// operation and tile mode.  All index arithmetic folds to constants or
+// shifts, each pass is inlined with exactly its own registers, and the
+// kernel is persistent with a two-stage shared-memory pipeline:
+//
+//   stage(it+1): cp.async 16/8/4-byte copies of the next tile's input into
+//                the other buffer (issued before the current tile's passes)
+//   pass 0:      reads the staged tile in its input layout (applying the
+//                real-transform pre-processing on the fly), writes the padded
+//                work layout
+//   pass 1..m-2: shared memory -> registers -> shared memory
+//   pass m-1:    registers -> global memory (coalesced), or -> shared memory
+//                followed by the real-transform post-process for R2C
+//
+// Phase functions are __host__ __device__ and take (tid, T) so the CPU
+// harness (tests/native/tile_emu.cpp) runs them thread by thread.
+#pragma once
+
+#include "fft_core.cuh"
+#include "sk_registry.h"
+#include "tile_io.cuh"
+
+namespace sipfft {
+
+template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int... Rs>
+struct SkCfg {
+    static constexpr int N = N_;
+    static constexpr int P = P_;
+    static constexpr int T = T_;
+    static constexpr int OP = OP_;
+    static constexpr int MODE = MODE_;
+    static constexpr int SIGN = SIGN_;
+    static constexpr bool TW4 = TW4_;
+    static constexpr int NP = sizeof...(Rs);
+
+    static constexpr int radix(int p) {
+        constexpr int r[] = {Rs...};
+        return r[p];
+    }
+    static constexpr int span(int p) {  // product of the radices before pass p
+        int l = 1;
+        for (int i = 0; i < p; ++i) l *= radix(i);
+        return l;
+    }
+    static constexpr int twoff(int p) {  // offset of pass p in the Stockham table
+        int off = 0;
+        for (int i = 0; i < p; ++i)
+            if (span(i) > 1) off += span(i) * (radix(i) - 1);
+        return off;
+    }
+    static constexpr bool colmap(int p) { return MODE == SK_COLS || (MODE == SK_ROWS_T && p == NP - 1); }
+    static constexpr int slots(int p) { return (P * (N / radix(p)) + T - 1) / T; }
+
+    // Work layout: element n of transform q at q * LD + sidx(n), LD odd.
+    static constexpr int LD = ((sidx(N - 1) + 1) & 1) ? sidx(N - 1) + 1 : sidx(N - 1) + 2;
+    // Staged input values (complex64 units) per tile.
+    static constexpr int STAGE = OP == OP_C2R_HALF ? P * (N + 1)
+                               : OP == OP_C2R_PAIR ? P * (N + 1)
+                               : P * N;  // R2C pair: 2P rows of N floats = P*N complex slots
+    static constexpr int BUF = (STAGE > P * LD ? STAGE : P * LD);  // complex values per buffer
+    static constexpr int SMEM = 2 * BUF * 8;
+    // CTAs per SM the shared memory allows with two stages (228 KB per SM,
+    // 1 KB reserved per CTA); used as the register-allocation target.
+    static constexpr int smem_ctas(int stages) {
+        const int per = stages * BUF * 8 + 1024;
+        const int n = (228 * 1024) / per;
+        return n < 1 ? 1 : n;
+    }
+    static constexpr int minb(int stages) {
+        int b = smem_ctas(stages);
+        const int thr = 2048 / T;          // thread limit per SM
+        const int regs = 65536 / (T * 64);  // keep >= 64 registers per thread
+        if (b > thr) b = thr;
+        if (b > regs) b = regs;
+        return b < 1 ? 1 : b;
+    }
+
+    static_assert(span(NP) == N, "radices must multiply to N");
+    static_assert(OP != OP_C2C || MODE != SK_COLS || true, "");
+    static_assert(!(TW4 && OP != OP_C2C), "cross twiddles are C2C only");
+};
+
+// ------------------------------------------------------------ staging
+// Copies the tile's input into `stage` (byte-exact image of the input
+// layout: rows [q][n] for the row modes, [n][q] for SK_COLS).
+SIP_HD void sk_copy_run(int tid, int T, float2* stage_base, int stage_off_bytes, const char* src, long long bytes) {
+    char* dst = reinterpret_cast<char*>(stage_base) + stage_off_bytes;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const int g = ((a | (uintptr_t)bytes | (uintptr_t)stage_off_bytes) & 15) == 0 ? 16
+                : ((a | (uintptr_t)bytes | (uintptr_t)stage_off_bytes) & 7) == 0 ? 8 : 4;
+    const long long chunks = bytes / g;
+    for (long long c = tid; c < chunks; c += T) {
+#if defined(__CUDA_ARCH__)
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + c * g);
+        if (g == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + c * g));
+        else if (g == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src + c * g));
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src + c * g));
+#else
+        for (int b = 0; b < g; ++b) dst[c * g + b] = src[c * g + b];
+#endif
+    }
+}
+
+template <class K>
+SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage) {
+    constexpr int T = K::T;
+    const char* src = static_cast<const char*>(a.src);
+    if constexpr (K::MODE == SK_COLS) {
+        // [n][q]: one run of cnt adjacent columns per element index n
+        const char* base = src + c.in_base * 8;
+        const long long pitch = a.in_stride * 8;
+        const uintptr_t align = reinterpret_cast<uintptr_t>(base) | (uintptr_t)pitch | (uintptr_t)(c.cnt * 8);
+        const int g = (align & 15) == 0 ? 16 : 8;
+        const int cpr = c.cnt * 8 / g;  // chunks per run
+        const int total = K::N * cpr;
+        char* dst = reinterpret_cast<char*>(stage);
+        for (int ch = tid; ch < total; ch += T) {
+            const int n = ch / cpr;
+            const int cc = ch - n * cpr;
+            const char* s = base + n * pitch + cc * g;
+            char* d = dst + n * (K::P * 8) + cc * g;
+#if defined(__CUDA_ARCH__)
+            const unsigned da = (unsigned)__cvta_generic_to_shared(d);
+            if (g == 16)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(da), "l"(s));
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(da), "l"(s));
+#else
+            for (int b = 0; b < g; ++b) d[b] = s[b];
+#endif
+        }
+    } else if constexpr (K::OP == OP_R2C_PAIR) {
+        const int r0 = 2 * c.i0;
+        const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
+        sk_copy_run(tid, T, stage, 0, src + (long long)r0 * a.in_idist * 4, (long long)nrows * K::N * 4);
+    } else if constexpr (K::OP == OP_C2R_PAIR) {
+        const int r0 = 2 * c.i0;
+        const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
+        sk_copy_run(tid, T, stage, 0, src + (long long)r0 * a.in_idist * 8, (long long)nrows * (K::N / 2 + 1) * 8);
+    } else {
+        const int rowlen = K::OP == OP_C2R_HALF ? K::N + 1 : K::N;
+        sk_copy_run(tid, T, stage, 0, src + c.in_base * 8, (long long)c.cnt * rowlen * 8);
+    }
+}
+
+// The partner of the last real row of an odd batch is zero (pair ops).
+template <class K>
+SIP_HD void sk_zero_missing(int tid, const TileArgs& a, const TileCtx& c, float2* stage) {
+    if constexpr (K::OP == OP_R2C_PAIR || K::OP == OP_C2R_PAIR) {
+        const int r0 = 2 * c.i0;
+        const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
+        if (nrows & 1) {
+            if constexpr (K::OP == OP_R2C_PAIR) {
+                float* s = reinterpret_cast<float*>(stage) + (long long)nrows * K::N;
+                for (int n = tid; n < K::N; n += K::T) s[n] = 0.f;
+            } else {
+                float2* s = stage + (long long)nrows * (K::N / 2 + 1);
+                for (int n = tid; n < K::N / 2 + 1; n += K::T) s[n] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+}
+
+// Value n of transform q as pass 0 reads it from the staged input.
+template <class K>
+SIP_HD float2 sk_input(const TileArgs& a, const float2* stage, int q, int n) {
+    constexpr int N = K::N;
+    if constexpr (K::OP == OP_C2C) {
+        const float2 v = K::MODE == SK_COLS ? stage[n * K::P + q] : stage[q * N + n];
+        return maybe_conj(v, (a.flags & TF_CONJ_IN) != 0);
+    } else if constexpr (K::OP == OP_R2C_HALF) {
+        return stage[q * N + n];
+    } else if constexpr (K::OP == OP_R2C_PAIR) {
+        const float* s = reinterpret_cast<const float*>(stage);
+        return make_float2(s[(2 * q) * N + n], s[(2 * q + 1) * N + n]);
+    } else if constexpr (K::OP == OP_C2R_HALF) {
+        // Z[n] = E + i W_{2M}^{+n} D from X[n], X[M-n] (DC / Nyquist use real parts only)
+        const float2* row = stage + q * (N + 1);
+        const bool cj = (a.flags & TF_CONJ_IN) != 0;
+        if (n == 0) {
+            const float dc = row[0].x, ny = row[N].x;
+            return make_float2(0.5f * (dc + ny), 0.5f * (dc - ny));
+        }
+        const float2 x = maybe_conj(row[n], cj), y = maybe_conj(row[N - n], cj);
+        const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
+        const float2 od = c_mulc(d, SIP_LDG(a.tw2 + n));
+        return make_float2(e.x - od.y, e.y + od.x);
+    } else {  // OP_C2R_PAIR
+        constexpr int H = N / 2 + 1;
+        const int kk = n <= N / 2 ? n : N - n;
+        float2 xa = stage[(2 * q) * H + kk];
+        float2 xb = stage[(2 * q + 1) * H + kk];
+        if (kk == 0 || 2 * kk == N) {
+            xa.y = 0.f;
+            xb.y = 0.f;
+        }
+        if ((n > N / 2) != ((a.flags & TF_CONJ_IN) != 0)) {
+            xa.y = -xa.y;
+            xb.y = -xb.y;
+        }
+        return make_float2(xa.x - xb.y, xa.y + xb.x);
+    }
+}
+
+// ------------------------------------------------------------- passes
+template <class K, int PASS>
+struct SkPass {
+    static constexpr int R = K::radix(PASS);
+    static constexpr int L = K::span(PASS);
+    static constexpr int NR = K::N / R;
+    static constexpr int S = K::slots(PASS);
+    static constexpr int TOTAL = K::P * NR;
+    static constexpr bool COL = K::colmap(PASS);
+    static constexpr bool LAST = PASS == K::NP - 1;
+    using Regs = PassRegs<R, S>;
+
+    SIP_HD static void butterfly_index(int b, int& q, int& j) {
+        if (COL) {
+            q = b % K::P;
+            j = b / K::P;
+        } else {
+            q = b / NR;
+            j = b % NR;
+        }
+    }
+
+    // Reads (pass 0: from the staged input) and transforms this thread's butterflies.
+    SIP_HD static void read(int tid, const TileArgs& a, const float2* buf, Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int b = tid + s * K::T;
+            if (TOTAL % K::T == 0 || b < TOTAL) {
+                int q, j;
+                butterfly_index(b, q, j);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if constexpr (PASS == 0)
+                        rg.v[s][r] = sk_input<K>(a, buf, q, j + r * NR);
+                    else
+                        rg.v[s][r] = buf[q * K::LD + sidx(j + r * NR)];
+                }
+                if constexpr (L > 1) {
+                    const int k = j % L;
+                    const float2* w = a.tw + K::twoff(PASS) + k * (R - 1);
+#pragma unroll
+                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + r - 1));
+                }
+                dft<R, K::SIGN>(rg.v[s]);
+            }
+        }
+    }
+
+    // Writes to the padded work layout (all passes except a global-storing last one).
+    SIP_HD static void write_smem(int tid, float2* buf, const Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int b = tid + s * K::T;
+            if (TOTAL % K::T == 0 || b < TOTAL) {
+                int q, j;
+                butterfly_index(b, q, j);
+                const int o = (j / L) * L * R + j % L;
+#pragma unroll
+                for (int r = 0; r < R; ++r) buf[q * K::LD + sidx(o + r * L)] = rg.v[s][r];
+            }
+        }
+    }
+
+    // Last pass straight to global memory: element k = j + r N/R of transform q.
+    SIP_HD static void write_global(int tid, const TileArgs& a, const TileCtx& c, const Regs& rg) {
+        static_assert(LAST, "global store from the last pass only");
+        const bool sc = (a.flags & TF_SCALE) != 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int b = tid + s * K::T;
+            if (TOTAL % K::T == 0 || b < TOTAL) {
+                int q, j;
+                butterfly_index(b, q, j);
+                if (q >= c.cnt) continue;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int k = j + r * NR;
+                    float2 v = rg.v[s][r];
+                    if constexpr (K::OP == OP_C2C) {
+                        if constexpr (K::TW4) v = c_tw<K::SIGN>(v, SIP_LDG(a.tw2 + (long long)(c.i0 + q) * k));
+                        if (sc) v = c_scale(v, a.scale);
+                        v = maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
+                        static_cast<float2*>(a.dst)[c.out_base + (long long)q * a.out_idist + (long long)k * a.out_stride] = v;
+                    } else if constexpr (K::OP == OP_C2R_HALF) {
+                        const float f = 2.0f * (sc ? a.scale : 1.0f);
+                        static_cast<float2*>(a.dst)[c.out_base + (long long)q * a.out_idist + k] = c_scale(v, f);
+                    } else if constexpr (K::OP == OP_C2R_PAIR) {
+                        const float f = sc ? a.scale : 1.0f;
+                        const int row = 2 * (c.i0 + q);
+                        float* d = static_cast<float*>(a.dst);
+                        d[(long long)row * a.out_idist + k] = v.x * f;
+                        if (row + 1 < a.rows) d[(long long)(row + 1) * a.out_idist + k] = v.y * f;
+                    }
+                }
+            }
+        }
+    }
+};
+
+template <class K>
+constexpr bool sk_last_to_smem() {
+    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR;
+}
+
+}  // namespace sipfft
+
+// ------------------------------------------------------------ kernel
+#if defined(__CUDACC__)
+namespace sipfft {
+
+extern __shared__ __align__(16) float2 sk_smem[];
+
+__device__ __forceinline__ void sk_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void sk_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+template <class K, int PASS>
+__device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
+    using SP = SkPass<K, PASS>;
+    typename SP::Regs rg;
+    SP::read(tid, a, buf, rg);
+    if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
+        SP::write_global(tid, a, c, rg);
+    } else {
+        __syncthreads();
+        SP::write_smem(tid, buf, rg);
+        __syncthreads();
+        if constexpr (!SP::LAST) sk_run<K, PASS + 1>(tid, a, c, buf);
+    }
+}
+
+// STAGES = 2: the next tile is staged while the current one is transformed;
+// STAGES = 1: one buffer (tiles too large to double), overlap comes from
+// several CTAs per SM.
+template <class K, int STAGES>
+__global__ void __launch_bounds__(K::T, K::minb(STAGES)) sk_fft_kernel(const TileArgs a) {
+    const int tid = threadIdx.x;
+    float2* bufs[2] = {sk_smem, sk_smem + (STAGES == 2 ? K::BUF : 0)};
+    int tile = blockIdx.x;
+    if (tile >= a.ntiles) return;
+    if (STAGES == 2) {
+        sk_stage<K>(tid, a, decode_tile(a, tile), bufs[0]);
+        sk_commit();
+    }
+    for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
+        float2* cur = bufs[it & 1];
+        const TileCtx c = decode_tile(a, tile);
+        if (STAGES == 2) {
+            const int next = tile + gridDim.x;
+            if (next < a.ntiles) sk_stage<K>(tid, a, decode_tile(a, next), bufs[(it + 1) & 1]);
+            sk_commit();
+            sk_wait<1>();
+        } else {
+            sk_stage<K>(tid, a, c, cur);
+            sk_commit();
+            sk_wait<0>();
+        }
+        __syncthreads();
+        if constexpr (K::OP == OP_R2C_PAIR || K::OP == OP_C2R_PAIR) {
+            sk_zero_missing<K>(tid, a, c, cur);
+            __syncthreads();
+        }
+        sk_run<K, 0>(tid, a, c, cur);
+        if constexpr (K::OP == OP_R2C_HALF) store_r2c_half(tid, K::T, a, c, cur);
+        if constexpr (K::OP == OP_R2C_PAIR) store_r2c_pair(tid, K::T, a, c, cur);
+        __syncthreads();
+    }
+}
+
+}  // namespace sipfft
+#endif

@@ -1,0 +1,38 @@
+// Lookup of the size-specialized kernels compiled by the sk_shard units.
+#include "sk_configs.h"
+#include "sk_registry.h"
+
+namespace sipfft {
+
+void sk_register_shard_0(std::vector<SkEntry>&);
+void sk_register_shard_1(std::vector<SkEntry>&);
+void sk_register_shard_2(std::vector<SkEntry>&);
+void sk_register_shard_3(std::vector<SkEntry>&);
+void sk_register_shard_4(std::vector<SkEntry>&);
+void sk_register_shard_5(std::vector<SkEntry>&);
+void sk_register_shard_6(std::vector<SkEntry>&);
+void sk_register_shard_7(std::vector<SkEntry>&);
+
+const std::vector<SkEntry>& sk_registry() {
+    static const std::vector<SkEntry> reg = [] {
+        std::vector<SkEntry> v;
+        sk_register_shard_0(v);
+        sk_register_shard_1(v);
+        sk_register_shard_2(v);
+        sk_register_shard_3(v);
+        sk_register_shard_4(v);
+        sk_register_shard_5(v);
+        sk_register_shard_6(v);
+        sk_register_shard_7(v);
+        return v;
+    }();
+    return reg;
+}
+
+const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n) {
+    for (const SkEntry& e : sk_registry())
+        if (e.op == op && e.mode == mode && e.sign == sign && e.tw4 == tw4 && e.n == n) return &e;
+    return nullptr;
+}
+
+}  // namespace sipfft

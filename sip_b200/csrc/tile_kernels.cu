@@ -39,13 +39,25 @@ cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes) {
 }
 
 cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream) {
-    KernelFn fn = pick_kernel(L.sign, L.e, L.op, L.tw4);
-    if (fn == nullptr) return cudaErrorInvalidValue;
     TileArgs a = L.args;
     a.src = src;
     a.dst = dst;
+    if (L.sk_fn != nullptr) {
+        void* params[] = {&a};
+        return cudaLaunchKernel(L.sk_fn, dim3(L.grid), dim3(L.block), params, (size_t)L.smem_bytes, stream);
+    }
+    KernelFn fn = pick_kernel(L.sign, L.e, L.op, L.tw4);
+    if (fn == nullptr) return cudaErrorInvalidValue;
     fn<<<L.grid, L.block, L.smem_bytes, stream>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t sk_prepare(const void* fn, int smem_bytes, int block, int* ctas_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, block, (size_t)smem_bytes);
 }
 
 const void* tile_kernel_address(int sign, int e, int op, bool tw4) {

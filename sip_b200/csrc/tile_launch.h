@@ -21,6 +21,7 @@ struct TileLaunch {
     int grid = 0;
     int block = 0;
     int smem_bytes = 0;
+    const void* sk_fn = nullptr;  // size-specialized kernel (sk_configs.h), else the generic one
     TileArgs args{};  // src / dst are bound per exec
 };
 
@@ -28,6 +29,10 @@ struct TileLaunch {
 cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes);
 
 cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream);
+
+// Raises the shared-memory limits of a size-specialized kernel and reports
+// how many of its CTAs fit on one SM.
+cudaError_t sk_prepare(const void* fn, int smem_bytes, int block, int* ctas_per_sm);
 
 const void* tile_kernel_address(int sign, int e, int op, bool tw4);
 

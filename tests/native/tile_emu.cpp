@@ -11,6 +11,7 @@
 // phase wrote shows up in the result.  Twiddles are computed on the host
 // in long double and rounded once to float.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -18,6 +19,8 @@
 
 #include "plan.h"
 #include "real_math.cuh"
+#include "sk_configs.h"
+#include "sk_kernel.cuh"
 
 using namespace sipfft;
 
@@ -68,6 +71,81 @@ void emu_passes(int T, const TileArgs& a, float2* sm) {
     }
 }
 
+// ---- size-specialized kernels: the same SkPass phase functions per thread
+template <class K, int PASS>
+void emu_sk_passes(const TileArgs& a, const TileCtx& c, float2* buf) {
+    using SP = SkPass<K, PASS>;
+    std::vector<typename SP::Regs> regs(K::T);
+    for (int tid = 0; tid < K::T; ++tid) SP::read(tid, a, buf, regs[tid]);
+    if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
+        for (int tid = 0; tid < K::T; ++tid) SP::write_global(tid, a, c, regs[tid]);
+    } else {
+        for (int tid = 0; tid < K::T; ++tid) SP::write_smem(tid, buf, regs[tid]);
+        if constexpr (!SP::LAST) emu_sk_passes<K, PASS + 1>(a, c, buf);
+    }
+}
+
+template <class K>
+void emu_sk_run(const TileArgs& a) {
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    std::vector<float2> buf(K::BUF);
+    for (int tile = 0; tile < a.ntiles; ++tile) {
+        const TileCtx c = decode_tile(a, tile);
+        for (auto& v : buf) v = make_float2(nan, nan);
+        for (int tid = 0; tid < K::T; ++tid) sk_stage<K>(tid, a, c, buf.data());
+        for (int tid = 0; tid < K::T; ++tid) sk_zero_missing<K>(tid, a, c, buf.data());
+        emu_sk_passes<K, 0>(a, c, buf.data());
+        if constexpr (K::OP == OP_R2C_HALF)
+            for (int tid = 0; tid < K::T; ++tid) store_r2c_half(tid, K::T, a, c, buf.data());
+        if constexpr (K::OP == OP_R2C_PAIR)
+            for (int tid = 0; tid < K::T; ++tid) store_r2c_pair(tid, K::T, a, c, buf.data());
+    }
+}
+
+using EmuSkFn = void (*)(const TileArgs&);
+
+template <class K, int STAGES>
+SkEntry emu_entry(std::vector<int> radices) {
+    SkEntry e;
+    e.n = K::N;
+    e.P = K::P;
+    e.T = K::T;
+    e.op = K::OP;
+    e.mode = K::MODE;
+    e.sign = K::SIGN;
+    e.tw4 = K::TW4;
+    e.stages = STAGES;
+    e.radices = std::move(radices);
+    e.LD = K::LD;
+    e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8;
+    e.fn = reinterpret_cast<const void*>(&emu_sk_run<K>);
+    return e;
+}
+
+}  // namespace
+
+namespace sipfft {
+const std::vector<SkEntry>& sk_registry() {
+    static const std::vector<SkEntry> reg = [] {
+        std::vector<SkEntry> v;
+#define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, ...) \
+    v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
+        SIP_SK_CONFIGS(SIP_EMU_SK)
+#undef SIP_EMU_SK
+        return v;
+    }();
+    return reg;
+}
+const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n) {
+    if (std::getenv("SIP_EMU_GENERIC_ONLY")) return nullptr;
+    for (const SkEntry& e : sk_registry())
+        if (e.op == op && e.mode == mode && e.sign == sign && e.tw4 == tw4 && e.n == n) return &e;
+    return nullptr;
+}
+}  // namespace sipfft
+
+namespace {
+
 void emu_tile_step(const Step& st, const void* src, void* dst) {
     TileArgs a = st.L.args;
     a.src = src;
@@ -81,6 +159,10 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
     }
     a.tw = tw.data();
     a.tw2 = tw2.empty() ? nullptr : tw2.data();
+    if (st.sk != nullptr) {
+        reinterpret_cast<EmuSkFn>(const_cast<void*>(st.sk->fn))(a);
+        return;
+    }
     const int T = st.L.block;
     const float nan = std::numeric_limits<float>::quiet_NaN();
     std::vector<float2> smv((size_t)a.P * a.LD);
@@ -221,3 +303,20 @@ int emu_dft(int r, int sign, float* data) {
 }
 
 }  // extern "C"
+
+extern "C" {
+// Lists the compiled size-specialized configurations: 7 ints per entry
+// (op, mode, sign, tw4, n, P, T); returns the entry count.
+int emu_sk_list(int* out, int cap) {
+    const auto& reg = sipfft::sk_registry();
+    int i = 0;
+    for (const auto& e : reg) {
+        if (i < cap) {
+            int* o = out + 7 * i;
+            o[0] = e.op; o[1] = e.mode; o[2] = e.sign; o[3] = e.tw4 ? 1 : 0; o[4] = e.n; o[5] = e.P; o[6] = e.T;
+        }
+        ++i;
+    }
+    return i;
+}
+}

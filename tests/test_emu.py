@@ -87,3 +87,51 @@ def test_fastdiv_exact(emu):
     d = np.ascontiguousarray(np.concatenate([d, edge_d]))
     n = np.ascontiguousarray(np.concatenate([n, edge_n]))
     assert emu.emu_fastdiv_check(d.ctypes.data, n.ctypes.data, d.size) == 0
+
+
+def _sk_list(emu):
+    import ctypes
+
+    emu.emu_sk_list.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    buf = np.zeros(7 * 256, np.int32)
+    n = emu.emu_sk_list(buf.ctypes.data, 256)
+    return [tuple(int(v) for v in buf[7 * i:7 * i + 7]) for i in range(n)]
+
+
+def _plan_for_sk(op, mode, sign, tw4, n):
+    """(type, direction, sizes, batch) of a plan whose steps include this kernel."""
+    d = O.FORWARD if sign < 0 else O.INVERSE
+    if mode == 0:  # rows
+        if op == 0:
+            return O.C2C, d, [n], 37
+        if op == 1:
+            return O.R2C, O.INVERSE, [2 * n], 21
+        if op == 2:
+            return O.C2R, O.FORWARD, [2 * n], 21
+        if op == 3:
+            return O.R2C, O.FORWARD, [n], 9
+        return O.C2R, O.INVERSE, [n], 9
+    if mode == 1 and not tw4:
+        return O.C2C, d, [n, 24], 2
+    split = {256: 65536, 512: 1 << 19, 1024: 1 << 19}
+    return O.C2C, d, [split[n]], 1
+
+
+def test_every_specialized_kernel(emu):
+    """Each compiled size-specialized kernel is selected by the planner and
+    matches the FP64 oracle (including partial tiles and odd row counts)."""
+    entries = _sk_list(emu)
+    assert len(entries) >= 20
+    for op, mode, sign, tw4, n, P, T in entries:
+        typ, d, sizes, batch = _plan_for_sk(op, mode, sign, tw4, n)
+        x = random_input(typ, sizes, batch, seed=n + op)
+        rc, out, desc = emu_run(emu, typ, d, sizes, batch, x)
+        assert rc == 0, desc
+        import json
+
+        steps = json.loads(desc)["steps"]
+        hit = [s for s in steps if s.get("sk") and s["n"] == n and s["op"] == op and s["sign"] == sign
+               and s["tw4"] == bool(tw4)]
+        assert hit, (op, mode, sign, tw4, n, desc[:400])
+        err = O.rel_l2(out, O.fp64(typ, d, x, sizes))
+        assert err <= REL_L2_TOL, (op, mode, sign, tw4, n, err)
