@@ -24,7 +24,7 @@ void check(cudaError_t e, const char* what) {
 
 struct TableKey {
     int device;
-    int kind;  // 0 stockham, 1 roots
+    int kind;  // 0 stockham, 1 roots, 2 basis
     long long a, b;
     std::vector<int> radices;
     bool operator<(const TableKey& o) const {
@@ -69,6 +69,19 @@ BufPtr stockham_table(int device, const PlanDev& pd, const std::vector<int>& rad
     return b;
 }
 
+BufPtr basis_table(int device, const PlanDev& pd, const std::vector<int>& radices) {
+    const int entries = basis_entries(pd);
+    TableKey key{device, 2, pd.N, 0, radices};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    BufPtr b = alloc_buf((size_t)std::max(entries, 1) * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_basis_twiddles(static_cast<float2*>(b->ptr), pd, s); });
+    g_tables[key] = b;
+    return b;
+}
+
 BufPtr root_table(int device, long long n, long long count) {
     TableKey key{device, 1, n, count, {}};
     std::lock_guard<std::mutex> lk(g_table_mu);
@@ -92,7 +105,7 @@ void prepare_device(FftPlan& plan) {
             st.real.tw = static_cast<const float2*>(st.tw2->ptr);
             continue;
         }
-        st.tw = stockham_table(device, st.host_plan, st.radices);
+        st.tw = st.sk ? basis_table(device, st.host_plan, st.radices) : stockham_table(device, st.host_plan, st.radices);
         st.plan_dev = alloc_buf(sizeof(PlanDev), device);
         check(cudaMemcpy(st.plan_dev->ptr, &st.host_plan, sizeof(PlanDev), cudaMemcpyHostToDevice), "cudaMemcpy");
         st.L.args.plan = static_cast<const PlanDev*>(st.plan_dev->ptr);

@@ -379,6 +379,26 @@ SIP_HD void pass_write(int tid, int T, int P, float2* sm, int LD, const PassDesc
     }
 }
 
+// Twiddle basis of a radix: a pass with span L > 1 needs W^{r k} for
+// r < R.  Writing r = r_lo + a r_hi (r_lo < a), the "basis" table holds, per
+// k, the a - 1 values W^{r_lo k} followed by the R/a - 1 values
+// W^{a r_hi k}; every other twiddle is one product of two table entries.
+// a is the divisor of R that minimises the entry count (R itself for a
+// prime, which degenerates to the full table).
+constexpr int basis_split(int R) {
+    int best = R, cost = R - 1;
+    for (int d = 2; d < R; ++d)
+        if (R % d == 0 && (d - 1) + (R / d - 1) < cost) {
+            cost = (d - 1) + (R / d - 1);
+            best = d;
+        }
+    return best;
+}
+constexpr int basis_count(int R) {
+    const int a = basis_split(R);
+    return (a - 1) + (R / a - 1);
+}
+
 // The radices a plan may use; every entry has a compiled pass.
 #define SIP_FFT_FOR_EACH_RADIX(X) \
     X(2) X(3) X(4) X(5) X(7) X(8) X(9) X(10) X(11) X(13) X(15) X(16) X(17) X(19) X(25) X(27) X(32)

@@ -8,23 +8,32 @@ namespace sipfft {
 
 namespace {
 
+// One thread per pair (k, m - k), k in [0, m/2]: each value is read once.
 __global__ void k_real_post(const RealPassArgs a) {
+    const long long pairs = a.m / 2 + 1;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
         const float2* z = a.src + row * a.in_pitch;
         float2* x = a.dst + row * a.out_pitch;
-        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k <= a.m;
-             k += (long long)gridDim.x * blockDim.x)
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pairs;
+             k += (long long)gridDim.x * blockDim.x) {
             x[k] = real_post_elem(z, k, a.m, a.tw, a.conj != 0);
+            const long long km = a.m - k;
+            if (km != k) x[km] = real_post_elem(z, km, a.m, a.tw, a.conj != 0);
+        }
     }
 }
 
 __global__ void k_real_pre(const RealPassArgs a) {
+    const long long pairs = a.m / 2 + 1;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
         const float2* x = a.src + row * a.in_pitch;
         float2* z = a.dst + row * a.out_pitch;
-        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < a.m;
-             k += (long long)gridDim.x * blockDim.x)
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pairs;
+             k += (long long)gridDim.x * blockDim.x) {
             z[k] = real_pre_elem(x, k, a.m, a.tw, a.conj != 0);
+            const long long km = a.m - k;
+            if (km != k && km < a.m) z[km] = real_pre_elem(x, km, a.m, a.tw, a.conj != 0);
+        }
     }
 }
 
@@ -38,12 +47,12 @@ dim3 grid_for(long long per_row, long long rows, int block) {
 }  // namespace
 
 cudaError_t real_post(const RealPassArgs& a, cudaStream_t stream) {
-    k_real_post<<<grid_for(a.m + 1, a.rows, 256), 256, 0, stream>>>(a);
+    k_real_post<<<grid_for(a.m / 2 + 1, a.rows, 256), 256, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t real_pre(const RealPassArgs& a, cudaStream_t stream) {
-    k_real_pre<<<grid_for(a.m, a.rows, 256), 256, 0, stream>>>(a);
+    k_real_pre<<<grid_for(a.m / 2 + 1, a.rows, 256), 256, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -26,7 +26,7 @@
 
 namespace sipfft {
 
-template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int... Rs>
+template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int MINB_, int... Rs>
 struct SkCfg {
     static constexpr int N = N_;
     static constexpr int P = P_;
@@ -46,17 +46,21 @@ struct SkCfg {
         for (int i = 0; i < p; ++i) l *= radix(i);
         return l;
     }
-    static constexpr int twoff(int p) {  // offset of pass p in the Stockham table
+    static constexpr int twoff(int p) {  // offset of pass p in the basis twiddle table
         int off = 0;
         for (int i = 0; i < p; ++i)
-            if (span(i) > 1) off += span(i) * (radix(i) - 1);
+            if (span(i) > 1) off += span(i) * basis_count(radix(i));
         return off;
     }
+    static constexpr int tw_entries() { return twoff(NP); }
+    // Odd first radices write conflict-free unpadded; even ones need the pad.
+    static constexpr bool PAD = radix(0) % 2 == 0;
+    static constexpr int idx(int n) { return PAD ? sidx(n) : n; }
     static constexpr bool colmap(int p) { return MODE == SK_COLS || (MODE == SK_ROWS_T && p == NP - 1); }
     static constexpr int slots(int p) { return (P * (N / radix(p)) + T - 1) / T; }
 
-    // Work layout: element n of transform q at q * LD + sidx(n), LD odd.
-    static constexpr int LD = ((sidx(N - 1) + 1) & 1) ? sidx(N - 1) + 1 : sidx(N - 1) + 2;
+    // Work layout: element n of transform q at q * LD + idx(n), LD odd.
+    static constexpr int LD = ((idx(N - 1) + 1) & 1) ? idx(N - 1) + 1 : idx(N - 1) + 2;
     // Staged input values (complex64 units) per tile.
     static constexpr int STAGE = OP == OP_C2R_HALF ? P * (N + 1)
                                : OP == OP_C2R_PAIR ? P * (N + 1)
@@ -70,14 +74,9 @@ struct SkCfg {
         const int n = (228 * 1024) / per;
         return n < 1 ? 1 : n;
     }
-    static constexpr int minb(int stages) {
-        int b = smem_ctas(stages);
-        const int thr = 2048 / T;          // thread limit per SM
-        const int regs = 65536 / (T * 64);  // keep >= 64 registers per thread
-        if (b > thr) b = thr;
-        if (b > regs) b = regs;
-        return b < 1 ? 1 : b;
-    }
+    // Minimum resident CTAs per SM (register-allocation target), chosen
+    // per configuration so that the kernel does not spill.
+    static constexpr int MINB = MINB_;
 
     static_assert(span(NP) == N, "radices must multiply to N");
     static_assert(OP != OP_C2C || MODE != SK_COLS || true, "");
@@ -245,13 +244,26 @@ struct SkPass {
                     if constexpr (PASS == 0)
                         rg.v[s][r] = sk_input<K>(a, buf, q, j + r * NR);
                     else
-                        rg.v[s][r] = buf[q * K::LD + sidx(j + r * NR)];
+                        rg.v[s][r] = buf[q * K::LD + K::idx(j + r * NR)];
                 }
                 if constexpr (L > 1) {
+                    // basis twiddles: W^{r k} = W^{r_lo k} W^{a r_hi k}
+                    constexpr int A = basis_split(R);
                     const int k = j % L;
-                    const float2* w = a.tw + K::twoff(PASS) + k * (R - 1);
+                    const float2* w = a.tw + K::twoff(PASS) + k * basis_count(R);
+                    float2 lo[A], hi[R / A];
+                    lo[0] = make_float2(1.f, 0.f);
+                    hi[0] = make_float2(1.f, 0.f);
 #pragma unroll
-                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + r - 1));
+                    for (int t = 1; t < A; ++t) lo[t] = SIP_LDG(w + t - 1);
+#pragma unroll
+                    for (int t = 1; t < R / A; ++t) hi[t] = SIP_LDG(w + A - 1 + t - 1);
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        const int rl = r % A, rh = r / A;
+                        const float2 t = rh == 0 ? lo[rl] : rl == 0 ? hi[rh] : c_mul(lo[rl], hi[rh]);
+                        rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], t);
+                    }
                 }
                 dft<R, K::SIGN>(rg.v[s]);
             }
@@ -268,7 +280,7 @@ struct SkPass {
                 butterfly_index(b, q, j);
                 const int o = (j / L) * L * R + j % L;
 #pragma unroll
-                for (int r = 0; r < R; ++r) buf[q * K::LD + sidx(o + r * L)] = rg.v[s][r];
+                for (int r = 0; r < R; ++r) buf[q * K::LD + K::idx(o + r * L)] = rg.v[s][r];
             }
         }
     }
@@ -314,6 +326,50 @@ constexpr bool sk_last_to_smem() {
     return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR;
 }
 
+// R2C post-process from the work layout (formulas of tile_io.cuh
+// store_r2c_half / store_r2c_pair), coalesced over the output rows.
+template <class K>
+SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* buf) {
+    const bool cj = (a.flags & TF_CONJ_OUT) != 0;
+    const bool sc = (a.flags & TF_SCALE) != 0;
+    float2* dst = static_cast<float2*>(a.dst);
+    if constexpr (K::OP == OP_R2C_HALF) {
+        constexpr int M = K::N, H = M + 1;
+        const int total = c.cnt * H;
+        for (int f = tid; f < total; f += K::T) {
+            const int q = f / H;
+            const int k = f - q * H;
+            const float2* row = buf + q * K::LD;
+            const float2 z = row[K::idx(k == M ? 0 : k)];
+            const float2 zm = row[K::idx(k == 0 ? 0 : M - k)];
+            const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            float2 x = c_add(ev, c_mul(SIP_LDG(a.tw2 + k), od));
+            if (sc) x = c_scale(x, a.scale);
+            dst[c.out_base + (long long)q * a.out_idist + k] = maybe_conj(x, cj);
+        }
+    } else if constexpr (K::OP == OP_R2C_PAIR) {
+        constexpr int N = K::N, H = N / 2 + 1;
+        const int r0 = 2 * c.i0;
+        const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
+        const int total = nrows * H;
+        for (int f = tid; f < total; f += K::T) {
+            const int rl = f / H;
+            const int k = f - rl * H;
+            const float2* row = buf + (rl >> 1) * K::LD;
+            const float2 z = row[K::idx(k)];
+            const float2 zm = row[K::idx(k == 0 ? 0 : N - k)];
+            float2 x;
+            if ((rl & 1) == 0)
+                x = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            else
+                x = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            if (sc) x = c_scale(x, a.scale);
+            dst[(long long)(r0 + rl) * a.out_idist + k] = maybe_conj(x, cj);
+        }
+    }
+}
+
 }  // namespace sipfft
 
 // ------------------------------------------------------------ kernel
@@ -347,7 +403,7 @@ __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx
 // STAGES = 1: one buffer (tiles too large to double), overlap comes from
 // several CTAs per SM.
 template <class K, int STAGES>
-__global__ void __launch_bounds__(K::T, K::minb(STAGES)) sk_fft_kernel(const TileArgs a) {
+__global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a) {
     const int tid = threadIdx.x;
     float2* bufs[2] = {sk_smem, sk_smem + (STAGES == 2 ? K::BUF : 0)};
     int tile = blockIdx.x;
@@ -375,8 +431,7 @@ __global__ void __launch_bounds__(K::T, K::minb(STAGES)) sk_fft_kernel(const Til
             __syncthreads();
         }
         sk_run<K, 0>(tid, a, c, cur);
-        if constexpr (K::OP == OP_R2C_HALF) store_r2c_half(tid, K::T, a, c, cur);
-        if constexpr (K::OP == OP_R2C_PAIR) store_r2c_pair(tid, K::T, a, c, cur);
+        if constexpr (sk_last_to_smem<K>()) sk_post<K>(tid, a, c, cur);
         __syncthreads();
     }
 }

@@ -33,9 +33,9 @@ SkEntry make_entry(std::vector<int> radices) {
 
 template <int SHARD>
 void register_shard(std::vector<SkEntry>& out) {
-#define SIP_SK_ENTRY(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, ...)                                     \
-    if constexpr (S == SHARD) {                                                                        \
-        out.push_back(make_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, __VA_ARGS__>, STAGES>({__VA_ARGS__})); \
+#define SIP_SK_ENTRY(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, ...)                                  \
+    if constexpr (S == SHARD) {                                                                              \
+        out.push_back(make_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, __VA_ARGS__>, STAGES>({__VA_ARGS__})); \
     }
     SIP_SK_CONFIGS(SIP_SK_ENTRY)
 #undef SIP_SK_ENTRY

@@ -42,6 +42,10 @@ const void* tile_kernel_address(int sign, int e, int op, bool tw4);
 // Stockham table for the pass list of `plan` (entries plan.N - 1 at most).
 cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries, cudaStream_t stream);
 
+// Basis table of the size-specialized kernels (entries: basis_entries).
+int basis_entries(const PlanDev& plan);
+cudaError_t gen_basis_twiddles(float2* out, const PlanDev& plan, cudaStream_t stream);
+
 // out[k] = exp(-2 pi i k / n), k in [0, count).
 cudaError_t gen_root_twiddles(float2* out, long long n, long long count, cudaStream_t stream);
 

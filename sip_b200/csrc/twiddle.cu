@@ -38,6 +38,29 @@ __global__ void k_stockham_tw(float2* out, const PlanDev plan, int entries) {
     }
 }
 
+// Basis table (fft_core.cuh basis_split): per pass with span L > 1 and per
+// k < L, W_{LR}^{r k} for r = 1..a-1, then W_{LR}^{a h k} for h = 1..R/a-1.
+__global__ void k_basis_tw(float2* out, const PlanDev plan, int entries) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= entries) return;
+    int off = 0;
+    for (int p = 0; p < plan.npass; ++p) {
+        const PassDesc& pd = plan.pass[p];
+        if (pd.L <= 1) continue;
+        const int bc = basis_count(pd.R);
+        const int cnt = pd.L * bc;
+        if (i < off + cnt) {
+            const int k = (i - off) / bc;
+            const int t = (i - off) - k * bc;
+            const int a = basis_split(pd.R);
+            const long long r = t < a - 1 ? t + 1 : (long long)a * (t - (a - 1) + 1);
+            out[i] = root_fwd(r * k, (long long)pd.L * pd.R);
+            return;
+        }
+        off += cnt;
+    }
+}
+
 __global__ void k_root_tw(float2* out, long long n, long long count) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x)
@@ -50,6 +73,21 @@ cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries,
     if (entries <= 0) return cudaSuccess;
     const int block = 256;
     k_stockham_tw<<<(entries + block - 1) / block, block, 0, stream>>>(out, plan, entries);
+    return cudaGetLastError();
+}
+
+int basis_entries(const PlanDev& plan) {
+    int n = 0;
+    for (int p = 0; p < plan.npass; ++p)
+        if (plan.pass[p].L > 1) n += plan.pass[p].L * basis_count(plan.pass[p].R);
+    return n;
+}
+
+cudaError_t gen_basis_twiddles(float2* out, const PlanDev& plan, cudaStream_t stream) {
+    const int entries = basis_entries(plan);
+    if (entries <= 0) return cudaSuccess;
+    const int block = 256;
+    k_basis_tw<<<(entries + block - 1) / block, block, 0, stream>>>(out, plan, entries);
     return cudaGetLastError();
 }
 

@@ -47,6 +47,24 @@ std::vector<float2> stockham_host(const PlanDev& pd) {
     return t;
 }
 
+// Basis twiddle table of the size-specialized kernels (fft_core.cuh basis_split).
+std::vector<float2> basis_host(const std::vector<int>& radices) {
+    std::vector<float2> t;
+    int L = 1;
+    for (int R : radices) {
+        if (L > 1) {
+            const int a = basis_split(R);
+            for (int k = 0; k < L; ++k) {
+                for (int r = 1; r < a; ++r) t.push_back(root_host((long long)r * k, (long long)L * R));
+                for (int h = 1; h < R / a; ++h) t.push_back(root_host((long long)a * h * k, (long long)L * R));
+            }
+        }
+        L *= R;
+    }
+    if (t.empty()) t.push_back(make_float2(1.f, 0.f));
+    return t;
+}
+
 template <int R, int SIGN, int S>
 void emu_pass(int T, const TileArgs& a, float2* sm, const PassDesc& pd) {
     std::vector<PassRegs<R, S>> regs(T);
@@ -95,10 +113,8 @@ void emu_sk_run(const TileArgs& a) {
         for (int tid = 0; tid < K::T; ++tid) sk_stage<K>(tid, a, c, buf.data());
         for (int tid = 0; tid < K::T; ++tid) sk_zero_missing<K>(tid, a, c, buf.data());
         emu_sk_passes<K, 0>(a, c, buf.data());
-        if constexpr (K::OP == OP_R2C_HALF)
-            for (int tid = 0; tid < K::T; ++tid) store_r2c_half(tid, K::T, a, c, buf.data());
-        if constexpr (K::OP == OP_R2C_PAIR)
-            for (int tid = 0; tid < K::T; ++tid) store_r2c_pair(tid, K::T, a, c, buf.data());
+        if constexpr (sk_last_to_smem<K>())
+            for (int tid = 0; tid < K::T; ++tid) sk_post<K>(tid, a, c, buf.data());
     }
 }
 
@@ -128,8 +144,8 @@ namespace sipfft {
 const std::vector<SkEntry>& sk_registry() {
     static const std::vector<SkEntry> reg = [] {
         std::vector<SkEntry> v;
-#define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, ...) \
-    v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
+#define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, ...) \
+    v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
         SIP_SK_CONFIGS(SIP_EMU_SK)
 #undef SIP_EMU_SK
         return v;
@@ -151,7 +167,7 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
     a.src = src;
     a.dst = dst;
     a.plan = &st.host_plan;
-    std::vector<float2> tw = stockham_host(st.host_plan);
+    std::vector<float2> tw = st.sk ? basis_host(st.radices) : stockham_host(st.host_plan);
     std::vector<float2> tw2;
     if (st.tw2_kind == 1) {
         tw2.resize(st.tw2_count);
