@@ -24,7 +24,7 @@ void check(cudaError_t e, const char* what) {
 
 struct TableKey {
     int device;
-    int kind;  // 0 stockham, 1 roots, 2 basis
+    int kind;  // 0 stockham, 1 roots, 2 basis, 3 split cross twiddles
     long long a, b;
     std::vector<int> radices;
     bool operator<(const TableKey& o) const {
@@ -94,6 +94,20 @@ BufPtr root_table(int device, long long n, long long count) {
     return b;
 }
 
+BufPtr split_table(int device, long long n, int shift) {
+    const long long B = 1LL << shift;
+    const long long count = B + (n + B - 1) / B;
+    TableKey key{device, 3, n, shift, {}};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    BufPtr b = alloc_buf((size_t)count * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_split_twiddles(static_cast<float2*>(b->ptr), n, shift, s); });
+    g_tables[key] = b;
+    return b;
+}
+
 }  // namespace
 
 void prepare_device(FftPlan& plan) {
@@ -101,11 +115,13 @@ void prepare_device(FftPlan& plan) {
     check(cudaGetDevice(&device), "cudaGetDevice");
     for (Step& st : plan.steps) {
         if (st.tw2_kind == 1) st.tw2 = root_table(device, st.tw2_n, st.tw2_count);
+        if (st.tw2_kind == 2) st.tw2 = split_table(device, st.tw2_n, st.L.args.tw4_shift);
         if (st.kind != StepKind::Tile) {
             st.real.tw = static_cast<const float2*>(st.tw2->ptr);
             continue;
         }
-        st.tw = st.sk ? basis_table(device, st.host_plan, st.radices) : stockham_table(device, st.host_plan, st.radices);
+        st.tw = (st.sk && st.sk->twb) ? basis_table(device, st.host_plan, st.radices)
+                                      : stockham_table(device, st.host_plan, st.radices);
         st.plan_dev = alloc_buf(sizeof(PlanDev), device);
         check(cudaMemcpy(st.plan_dev->ptr, &st.host_plan, sizeof(PlanDev), cudaMemcpyHostToDevice), "cudaMemcpy");
         st.L.args.plan = static_cast<const PlanDev*>(st.plan_dev->ptr);

@@ -316,9 +316,14 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
     a.out_stride = n2;
     Step sa = make_tile_step(OP_C2C, sign, n1, n1, true, a, 0, 0,
                              "four-step A n=" + std::to_string(n) + " n1=" + std::to_string(n1), true);
-    sa.tw2_kind = 1;
-    sa.tw2_n = n;
-    sa.tw2_count = n;
+    {
+        int shift = 0;
+        while ((1LL << (2 * shift)) < n) ++shift;  // B = 2^shift >= sqrt(n)
+        sa.L.args.tw4_shift = shift;
+        sa.tw2_kind = 2;
+        sa.tw2_n = n;
+        sa.tw2_count = (1LL << shift) + (n + (1LL << shift) - 1) / (1LL << shift);
+    }
     sa.src = o.src;
     sa.src_off = o.src_off;
     sa.dst = Loc::Ws;
@@ -379,14 +384,121 @@ void add_real_rows(FftPlan& plan, bool r2c, long long n, long long rows, Loc src
 
 bool real_fits_tile(long long n) { return (n % 2 == 0) ? n / 2 <= kMaxTileN : n <= kMaxTileN; }
 
-// Even real length whose half-length FFT needs the four-step split: the
-// complex four-step over the workspace plus an element-wise pre/post pass.
-// Workspace: [0, zbytes) four-step scratch, [zoff, zoff + zbytes) Z.
+// Step of a mirrored four-step kernel (OP_R2C_4B / OP_C2R_4A), which only
+// exist size-specialized: `e` is its registry entry.
+Step mirrored_step(const SkEntry* e, int n, int n_other, long long rows, const AxisIO& io, int flags,
+                   long long tw_n, const std::string& what) {
+    Step st;
+    st.sk = e;
+    st.radices = e->radices;
+    int tw_entries = 0;
+    st.host_plan = make_plandev(n, st.radices, &tw_entries);
+    TileLaunch& L = st.L;
+    L.sign = e->sign;
+    L.op = e->op;
+    L.block = e->T;
+    L.smem_bytes = e->smem;
+    TileArgs& a = L.args;
+    a.N = n;
+    a.P = e->P / 2;  // first-half rows / columns per tile; the mirrors fill the other half
+    a.LD = e->LD;
+    a.n_other = n_other;
+    a.inner = n_other / 2 + 1;
+    a.tiles_per_outer = (a.inner + a.P - 1) / a.P;
+    a.ntiles = (int)((long long)a.tiles_per_outer * rows);
+    a.in_odist = io.in_odist;
+    a.in_idist = io.in_idist;
+    a.in_stride = io.in_stride;
+    a.out_odist = io.out_odist;
+    a.out_idist = io.out_idist;
+    a.out_stride = io.out_stride;
+    a.flags = flags;
+    a.scale = 1.0f;
+    a.div_n = make_fastdiv((uint32_t)n);
+    a.div_p = make_fastdiv((uint32_t)a.P);
+    a.div_h = make_fastdiv((uint32_t)(n / 2 + 1));
+    a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+    int shift = 0;
+    while ((1LL << (2 * shift)) < tw_n) ++shift;
+    a.tw4_shift = shift;
+    st.tw2_kind = 2;
+    st.tw2_n = tw_n;
+    st.tw2_count = (1LL << shift) + (tw_n + (1LL << shift) - 1) / (1LL << shift);
+    L.grid = a.ntiles;
+    st.what = what + " [sk mirrored P=" + std::to_string(e->P) + "]";
+    return st;
+}
+
+// Even real length whose half-length FFT M needs the four-step split.
+// Fused form (both mirrored kernels compiled for the split): R2C = column
+// pass A + row pass B with the post-process on mirrored row pairs; C2R =
+// column pass A with the pre-process on mirrored column pairs + row pass B.
+// Otherwise: the complex four-step over the workspace plus an element-wise
+// pre/post pass.  Workspace: [0, zbytes) four-step scratch, then Z.
 void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     if (n % 2 != 0)
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "odd real length " + std::to_string(n) + " above one tile");
     const long long m = n / 2;
     const size_t zbytes = (size_t)(rows * m * 8);
+    int n1 = 0, n2 = 0;
+    const bool split = four_step_split(m, &n1, &n2);
+    const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr;
+    if (split && !generic_only) {
+        const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1) : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1);
+        const SkEntry* eb = r2c ? sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2) : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
+        if (ea != nullptr && eb != nullptr) {
+            if (r2c) {
+                C2COpts o;
+                o.sign = -1;
+                o.src = Loc::In;
+                o.dst = Loc::Out;  // replaced: pass B below
+                add_c2c_1d(plan, m, rows, o);
+                plan.steps.pop_back();  // keep pass A (column FFTs + cross twiddles) only
+                AxisIO io;
+                io.in_odist = m;
+                io.in_idist = n2;
+                io.in_stride = 1;
+                io.out_odist = m + 1;
+                io.out_idist = 1;
+                io.out_stride = n1;
+                Step sb = mirrored_step(eb, n2, n1, rows, io, plan.forward() ? 0 : TF_CONJ_OUT, 2 * m,
+                                        "r2c four-step B + post n=" + std::to_string(n));
+                sb.src = Loc::Ws;
+                sb.dst = Loc::Out;
+                plan.steps.push_back(sb);
+            } else {
+                AxisIO io;
+                io.in_odist = m + 1;
+                io.in_idist = 1;
+                io.in_stride = n2;
+                io.out_odist = m;
+                io.out_idist = 1;
+                io.out_stride = n2;
+                Step sa = mirrored_step(ea, n1, n2, rows, io, plan.forward() ? TF_CONJ_IN : 0, 2 * m,
+                                        "c2r pre + four-step A n=" + std::to_string(n));
+                sa.src = Loc::In;
+                sa.dst = Loc::Ws;
+                plan.steps.push_back(sa);
+                AxisIO b;
+                b.inner = n1;
+                b.outer = rows;
+                b.in_odist = m;
+                b.in_idist = n2;
+                b.in_stride = 1;
+                b.out_odist = m;
+                b.out_idist = 1;
+                b.out_stride = n1;
+                Step sb = make_tile_step(OP_C2C, 1, n2, n2, true, b, TF_SCALE, 0,
+                                         "four-step B n=" + std::to_string(m) + " n2=" + std::to_string(n2));
+                sb.L.args.scale = 2.0f;
+                sb.src = Loc::Ws;
+                sb.dst = Loc::Out;
+                plan.steps.push_back(sb);
+            }
+            plan.workspace_need = std::max(plan.workspace_need, zbytes);
+            return;
+        }
+    }
     const size_t zoff = (zbytes + 255) / 256 * 256;
     Step pp;
     pp.kind = r2c ? StepKind::RealPost : StepKind::RealPre;

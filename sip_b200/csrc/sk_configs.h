@@ -1,45 +1,49 @@
 // Compiled size-specialized tile kernels:
-//   X(shard, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, radices...)
+//   X(shard, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, radices...)
 // MINB is the CTAs-per-SM register target (__launch_bounds__), chosen so
-// that the kernel does not spill.
+// that the kernel does not spill.  TWB selects basis (1) or full (0) pass
+// twiddles (sk_kernel.cuh SkCfg::TWB).
 // Every other length runs on the generic tile kernel.  The shard index
 // spreads the instantiations over parallel compile units.
 #pragma once
 
 #define SIP_SK_CONFIGS(X)                                                     \
     /* 1D / last-axis C2C rows */                                             \
-    X(0, 4096, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 16, 16, 16)              \
-    X(1, 4096, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 16, 16, 16)               \
-    X(2, 2048, 2, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 16, 16, 8)               \
-    X(3, 2048, 2, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 16, 16, 8)                \
-    X(4, 1024, 4, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 16, 16, 4)               \
-    X(5, 1024, 4, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 16, 16, 4)                \
-    X(6, 256, 16, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 16, 16)                  \
-    X(7, 256, 16, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 16, 16)                   \
-    X(0, 8192, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 1, 32, 16, 16)              \
-    X(1, 8192, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 1, 32, 16, 16)               \
+    X(0, 4096, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 16)              \
+    X(1, 4096, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 16)               \
+    X(2, 2048, 2, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 8)               \
+    X(3, 2048, 2, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 8)                \
+    X(4, 1024, 4, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 4)               \
+    X(5, 1024, 4, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 4)                \
+    X(6, 256, 16, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16)                  \
+    X(7, 256, 16, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16)                   \
+    X(0, 8192, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 1, 1, 32, 16, 16)              \
+    X(1, 8192, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 1, 1, 32, 16, 16)               \
     /* strided axes of 2D / 3D transforms */                                  \
-    X(2, 2048, 8, 512, OP_C2C, SK_COLS, -1, false, 1, 1, 16, 16, 8)               \
-    X(3, 2048, 8, 512, OP_C2C, SK_COLS, 1, false, 1, 1, 16, 16, 8)                \
-    X(4, 256, 16, 256, OP_C2C, SK_COLS, -1, false, 2, 3, 16, 16)                  \
-    X(5, 256, 16, 256, OP_C2C, SK_COLS, 1, false, 2, 3, 16, 16)                   \
+    X(2, 2048, 8, 512, OP_C2C, SK_COLS, -1, false, 1, 1, 1, 16, 16, 8)               \
+    X(3, 2048, 8, 512, OP_C2C, SK_COLS, 1, false, 1, 1, 1, 16, 16, 8)                \
+    X(4, 256, 16, 256, OP_C2C, SK_COLS, -1, false, 2, 3, 1, 16, 16)                  \
+    X(5, 256, 16, 256, OP_C2C, SK_COLS, 1, false, 2, 3, 1, 16, 16)                   \
     /* four-step 65536 = 256 x 256 */                                         \
-    X(6, 256, 16, 256, OP_C2C, SK_COLS, -1, true, 2, 3, 16, 16)                   \
-    X(7, 256, 16, 256, OP_C2C, SK_COLS, 1, true, 2, 3, 16, 16)                    \
-    X(0, 256, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 16, 16)                \
-    X(1, 256, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 16, 16)                 \
+    X(6, 256, 16, 256, OP_C2C, SK_COLS, -1, true, 2, 3, 1, 16, 16)                   \
+    X(7, 256, 16, 256, OP_C2C, SK_COLS, 1, true, 2, 3, 1, 16, 16)                    \
+    X(0, 256, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 1, 16, 16)                \
+    X(1, 256, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 1, 16, 16)                 \
     /* four-step 2^19 = 512 x 1024 (real 2^20) */                             \
-    X(2, 512, 16, 256, OP_C2C, SK_COLS, -1, true, 1, 3, 16, 32)                   \
-    X(3, 512, 16, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 16, 32)                    \
-    X(4, 1024, 8, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 32, 32)                \
-    X(5, 1024, 8, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 32, 32)                 \
+    X(2, 512, 16, 256, OP_C2C, SK_COLS, -1, true, 1, 3, 1, 16, 32)                   \
+    X(3, 512, 16, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 1, 16, 32)                    \
+    X(4, 1024, 8, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 32, 32)                \
+    X(5, 1024, 8, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 32, 32)                 \
     /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000) */      \
-    X(6, 500, 8, 200, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 25, 20)              \
-    X(7, 500, 8, 200, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 25, 20)               \
-    X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 25, 15, 8)          \
-    X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 25, 15, 8)           \
+    X(6, 500, 8, 200, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 20)              \
+    X(7, 500, 8, 200, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 20)               \
+    X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 0, 25, 15, 8)          \
+    X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 0, 25, 15, 8)           \
     /* odd real length 2187 = 3^7, two rows per complex FFT */                \
-    X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 27, 9, 9)           \
-    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 27, 9, 9)
+    X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 0, 27, 9, 9)           \
+    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 0, 27, 9, 9)        \
+    /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A */      \
+    X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)      \
+    X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)
 
 #define SIP_SK_SHARDS 8

@@ -26,7 +26,7 @@
 
 namespace sipfft {
 
-template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int MINB_, int... Rs>
+template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int MINB_, int TWB_, int... Rs>
 struct SkCfg {
     static constexpr int N = N_;
     static constexpr int P = P_;
@@ -46,23 +46,37 @@ struct SkCfg {
         for (int i = 0; i < p; ++i) l *= radix(i);
         return l;
     }
-    static constexpr int twoff(int p) {  // offset of pass p in the basis twiddle table
+    // Pass twiddles: TWB = 1 reads the basis table (fft_core.cuh
+    // basis_split: fewer loads, one extra product), TWB = 0 the full
+    // Stockham table (one load per twiddle, fewer instructions).
+    static constexpr bool TWB = TWB_ != 0;
+    static constexpr int twcount(int r) { return TWB ? basis_count(r) : r - 1; }
+    static constexpr int twoff(int p) {  // offset of pass p in the twiddle table
         int off = 0;
         for (int i = 0; i < p; ++i)
-            if (span(i) > 1) off += span(i) * basis_count(radix(i));
+            if (span(i) > 1) off += span(i) * twcount(radix(i));
         return off;
     }
     static constexpr int tw_entries() { return twoff(NP); }
-    // Odd first radices write conflict-free unpadded; even ones need the pad.
+    // Odd first radices write conflict-free unpadded; even ones need a pad
+    // slot every max(16, R0) values (radix-32 strides need one per 32).
     static constexpr bool PAD = radix(0) % 2 == 0;
-    static constexpr int idx(int n) { return PAD ? sidx(n) : n; }
-    static constexpr bool colmap(int p) { return MODE == SK_COLS || (MODE == SK_ROWS_T && p == NP - 1); }
+    static constexpr int PADG = radix(0) > 16 ? radix(0) : 16;
+    static constexpr int idx(int n) { return PAD ? n + n / PADG : n; }
+    static constexpr bool colmap(int p) {
+        return MODE == SK_COLS || (MODE == SK_ROWS_T && p == NP - 1 && OP == OP_C2C);
+    }
+    // Mirrored-tile ops: slots [0, H) hold rows / columns c*H + q of the first
+    // half, slots [H, 2H) their mirrors (sk_mirror_*).
+    static constexpr bool MIRROR = OP == OP_R2C_4B || OP == OP_C2R_4A;
+    static constexpr int H = P / 2;
     static constexpr int slots(int p) { return (P * (N / radix(p)) + T - 1) / T; }
 
     // Work layout: element n of transform q at q * LD + idx(n), LD odd.
     static constexpr int LD = ((idx(N - 1) + 1) & 1) ? idx(N - 1) + 1 : idx(N - 1) + 2;
     // Staged input values (complex64 units) per tile.
     static constexpr int STAGE = OP == OP_C2R_HALF ? P * (N + 1)
+                               : (OP == OP_R2C_4B || OP == OP_C2R_4A) ? P * N
                                : OP == OP_C2R_PAIR ? P * (N + 1)
                                : P * N;  // R2C pair: 2P rows of N floats = P*N complex slots
     static constexpr int BUF = (STAGE > P * LD ? STAGE : P * LD);  // complex values per buffer
@@ -111,7 +125,7 @@ template <class K>
 SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage) {
     constexpr int T = K::T;
     const char* src = static_cast<const char*>(a.src);
-    if constexpr (K::MODE == SK_COLS) {
+    if constexpr (K::MODE == SK_COLS && !K::MIRROR) {
         // [n][q]: one run of cnt adjacent columns per element index n
         const char* base = src + c.in_base * 8;
         const long long pitch = a.in_stride * 8;
@@ -133,6 +147,55 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(da), "l"(s));
 #else
             for (int b = 0; b < g; ++b) d[b] = s[b];
+#endif
+        }
+    } else if constexpr (K::OP == OP_R2C_4B) {
+        // rows k1 = i0 + q (slot q) and N1 - k1 (slot H + q) of Y, N values each
+        const int n1 = a.n_other;
+        const char* ybase = src + (c.in_base - (long long)c.i0 * K::N) * 8;  // row 0 of this batch row
+        constexpr int CPR = K::N * 8 / 16;                                      // 16-byte chunks per row
+        for (int ch = tid; ch < K::P * CPR; ch += T) {
+            const int slot = ch / CPR;
+            const int cc = ch - slot * CPR;
+            const int q = slot < K::H ? slot : slot - K::H;
+            const int k1 = c.i0 + q;
+            if (q >= c.cnt) continue;
+            int row = k1;
+            if (slot >= K::H) {
+                if (k1 == 0 || 2 * k1 == n1) continue;  // self-mirrored rows
+                row = n1 - k1;
+            }
+            const char* s = ybase + (long long)row * K::N * 8 + cc * 16;
+            char* d = reinterpret_cast<char*>(stage) + slot * K::N * 8 + cc * 16;
+#if defined(__CUDA_ARCH__)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(d)),
+                         "l"(s));
+#else
+            for (int b = 0; b < 16; ++b) d[b] = s[b];
+#endif
+        }
+    } else if constexpr (K::OP == OP_C2R_4A) {
+        // element n1 of columns n2 = i0 + q (slot q) and N2 - n2 (slot H + q)
+        const int n2c = a.n_other;
+        const char* xbase = src + (c.in_base - c.i0) * 8;  // X[0] of this batch row
+        for (int e = tid; e < K::N * K::P; e += T) {
+            const int n1 = e / K::P;
+            const int slot = e - n1 * K::P;
+            const int q = slot < K::H ? slot : slot - K::H;
+            const int col0 = c.i0 + q;
+            if (q >= c.cnt) continue;
+            int col = col0;
+            if (slot >= K::H) {
+                if (col0 == 0 || 2 * col0 == n2c) continue;
+                col = n2c - col0;
+            }
+            const char* s = xbase + ((long long)n1 * n2c + col) * 8;
+            char* d = reinterpret_cast<char*>(stage) + (n1 * K::P + slot) * 8;
+#if defined(__CUDA_ARCH__)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(d)),
+                         "l"(s));
+#else
+            for (int b = 0; b < 8; ++b) d[b] = s[b];
 #endif
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
@@ -167,15 +230,62 @@ SIP_HD void sk_zero_missing(int tid, const TileArgs& a, const TileCtx& c, float2
     }
 }
 
+// Column index of slot q of a C2R_4A tile (-1 when the slot is unused).
+template <class K>
+SIP_HD int sk_c2r4a_col(const TileArgs& a, int i0, int cnt, int q) {
+    const int qq = q < K::H ? q : q - K::H;
+    if (qq >= cnt) return -1;
+    const int col0 = i0 + qq;
+    if (q < K::H) return col0;
+    if (col0 == 0 || 2 * col0 == a.n_other) return -1;
+    return a.n_other - col0;
+}
+
+// C2R_4A pass-0 input: Z[k] = E + i W_{2M}^{+k} D, k = n1 N2 + n2, from X[k]
+// and X[M-k] (M = N1 N2; the partner sits in the mirror column, row
+// N1-1-n1, or in the same column for n2 = 0 and n2 = N2/2; X[M] itself is
+// read from global memory).  The split table a.tw2 holds W_{2M}.
+template <class K>
+SIP_HD float2 sk_c2r4a_input(const TileArgs& a, const TileCtx& c, const float2* stage, int slot, int n1) {
+    const int n2c = a.n_other;
+    const int col = sk_c2r4a_col<K>(a, c.i0, c.cnt, slot);
+    if (col < 0) return make_float2(0.f, 0.f);
+    const long long M = (long long)K::N * n2c;
+    const bool cj = (a.flags & TF_CONJ_IN) != 0;
+    float2 x = maybe_conj(stage[n1 * K::P + slot], cj);
+    float2 y;
+    if (col == 0) {
+        if (n1 == 0) {
+            const float2* xrow = static_cast<const float2*>(a.src) + (c.in_base - c.i0);
+            const float ny = SIP_LDG(xrow + M).x;
+            return make_float2(0.5f * (x.x + ny), 0.5f * (x.x - ny));
+        }
+        y = stage[(K::N - n1) * K::P + slot];
+    } else if (2 * col == n2c) {
+        y = stage[(K::N - 1 - n1) * K::P + slot];
+    } else {
+        const int ms = slot < K::H ? slot + K::H : slot - K::H;
+        y = stage[(K::N - 1 - n1) * K::P + ms];
+    }
+    y = maybe_conj(y, cj);
+    const long long kk = (long long)n1 * n2c + col;
+    const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+    const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
+    const float2 od = c_mulc(d, cross_tw(a, kk));
+    return make_float2(e.x - od.y, e.y + od.x);
+}
+
 // Value n of transform q as pass 0 reads it from the staged input.
 template <class K>
-SIP_HD float2 sk_input(const TileArgs& a, const float2* stage, int q, int n) {
+SIP_HD float2 sk_input(const TileArgs& a, const TileCtx& c, const float2* stage, int q, int n) {
     constexpr int N = K::N;
     if constexpr (K::OP == OP_C2C) {
         const float2 v = K::MODE == SK_COLS ? stage[n * K::P + q] : stage[q * N + n];
         return maybe_conj(v, (a.flags & TF_CONJ_IN) != 0);
-    } else if constexpr (K::OP == OP_R2C_HALF) {
+    } else if constexpr (K::OP == OP_R2C_HALF || K::OP == OP_R2C_4B) {
         return stage[q * N + n];
+    } else if constexpr (K::OP == OP_C2R_4A) {
+        return sk_c2r4a_input<K>(a, c, stage, q, n);
     } else if constexpr (K::OP == OP_R2C_PAIR) {
         const float* s = reinterpret_cast<const float*>(stage);
         return make_float2(s[(2 * q) * N + n], s[(2 * q + 1) * N + n]);
@@ -232,7 +342,7 @@ struct SkPass {
     }
 
     // Reads (pass 0: from the staged input) and transforms this thread's butterflies.
-    SIP_HD static void read(int tid, const TileArgs& a, const float2* buf, Regs& rg) {
+    SIP_HD static void read(int tid, const TileArgs& a, const TileCtx& c, const float2* buf, Regs& rg) {
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const int b = tid + s * K::T;
@@ -242,11 +352,16 @@ struct SkPass {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if constexpr (PASS == 0)
-                        rg.v[s][r] = sk_input<K>(a, buf, q, j + r * NR);
+                        rg.v[s][r] = sk_input<K>(a, c, buf, q, j + r * NR);
                     else
                         rg.v[s][r] = buf[q * K::LD + K::idx(j + r * NR)];
                 }
-                if constexpr (L > 1) {
+                if constexpr (L > 1 && !K::TWB) {
+                    const int k = j % L;
+                    const float2* w = a.tw + K::twoff(PASS) + k * (R - 1);
+#pragma unroll
+                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + r - 1));
+                } else if constexpr (L > 1) {
                     // basis twiddles: W^{r k} = W^{r_lo k} W^{a r_hi k}
                     constexpr int A = basis_split(R);
                     const int k = j % L;
@@ -295,16 +410,22 @@ struct SkPass {
             if (TOTAL % K::T == 0 || b < TOTAL) {
                 int q, j;
                 butterfly_index(b, q, j);
-                if (q >= c.cnt) continue;
+                if (!K::MIRROR && q >= c.cnt) continue;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int k = j + r * NR;
                     float2 v = rg.v[s][r];
                     if constexpr (K::OP == OP_C2C) {
-                        if constexpr (K::TW4) v = c_tw<K::SIGN>(v, SIP_LDG(a.tw2 + (long long)(c.i0 + q) * k));
+                        if constexpr (K::TW4) v = c_tw<K::SIGN>(v, cross_tw(a, (long long)(c.i0 + q) * k));
                         if (sc) v = c_scale(v, a.scale);
                         v = maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
                         static_cast<float2*>(a.dst)[c.out_base + (long long)q * a.out_idist + (long long)k * a.out_stride] = v;
+                    } else if constexpr (K::OP == OP_C2R_4A) {
+                        const int col = sk_c2r4a_col<K>(a, c.i0, c.cnt, q);
+                        if (col < 0) continue;
+                        v = c_tw<K::SIGN>(v, cross_tw(a, 2LL * col * k));
+                        if (sc) v = c_scale(v, a.scale);
+                        static_cast<float2*>(a.dst)[c.out_base - c.i0 + col + (long long)k * a.out_stride] = v;
                     } else if constexpr (K::OP == OP_C2R_HALF) {
                         const float f = 2.0f * (sc ? a.scale : 1.0f);
                         static_cast<float2*>(a.dst)[c.out_base + (long long)q * a.out_idist + k] = c_scale(v, f);
@@ -323,7 +444,17 @@ struct SkPass {
 
 template <class K>
 constexpr bool sk_last_to_smem() {
-    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR;
+    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR || K::OP == OP_R2C_4B;
+}
+
+// R2C value X[k] from Z[k] and Z[M-k] (formula of tile_io.cuh
+// store_r2c_half) with W_{2M}^k from the split table.
+SIP_HD float2 sk_r2c_value(const TileArgs& a, float2 z, float2 zm, long long k) {
+    const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+    const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+    float2 x = c_add(ev, c_mul(cross_tw(a, k), od));
+    if (a.flags & TF_SCALE) x = c_scale(x, a.scale);
+    return maybe_conj(x, (a.flags & TF_CONJ_OUT) != 0);
 }
 
 // R2C post-process from the work layout (formulas of tile_io.cuh
@@ -347,6 +478,34 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
             float2 x = c_add(ev, c_mul(SIP_LDG(a.tw2 + k), od));
             if (sc) x = c_scale(x, a.scale);
             dst[c.out_base + (long long)q * a.out_idist + k] = maybe_conj(x, cj);
+        }
+    } else if constexpr (K::OP == OP_R2C_4B) {
+        // rows k1 = i0 + q (slot q) and N1 - k1 (slot H + q) -> X[k1 + N1 k2]
+        // and X[(N1 - k1) + N1 (N2 - 1 - k2)]; row 0 and row N1/2 pair with
+        // themselves, row 0 also produces X[M].
+        constexpr int N2 = K::N;
+        const int N1 = a.n_other;
+        const long long M = (long long)N1 * N2;
+        float2* x = dst + (c.out_base - c.i0);
+        for (int f = tid; f < K::H * N2; f += K::T) {
+            const int q = f % K::H;
+            const int k2 = f / K::H;
+            if (q >= c.cnt) continue;
+            const int k1 = c.i0 + q;
+            const float2* rq = buf + q * K::LD;
+            const float2* rm = buf + (K::H + q) * K::LD;
+            const long long kk = k1 + (long long)N1 * k2;
+            const float2 z = rq[K::idx(k2)];
+            if (k1 == 0) {
+                x[kk] = sk_r2c_value(a, z, rq[K::idx(k2 == 0 ? 0 : N2 - k2)], kk);
+                if (k2 == 0) x[M] = sk_r2c_value(a, z, z, M);
+            } else if (2 * k1 == N1) {
+                x[kk] = sk_r2c_value(a, z, rq[K::idx(N2 - 1 - k2)], kk);
+            } else {
+                const float2 zm = rm[K::idx(N2 - 1 - k2)];
+                x[kk] = sk_r2c_value(a, z, zm, kk);
+                x[M - kk] = sk_r2c_value(a, zm, z, M - kk);
+            }
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
         constexpr int N = K::N, H = N / 2 + 1;
@@ -388,7 +547,7 @@ template <class K, int PASS>
 __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
     using SP = SkPass<K, PASS>;
     typename SP::Regs rg;
-    SP::read(tid, a, buf, rg);
+    SP::read(tid, a, c, buf, rg);
     if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
         SP::write_global(tid, a, c, rg);
     } else {

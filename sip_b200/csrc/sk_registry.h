@@ -14,6 +14,7 @@ enum SkMode : int {
 struct SkEntry {
     int n, P, T, op, mode, sign;
     bool tw4;
+    bool twb;  // basis pass twiddles (else the full Stockham table)
     int stages;
     std::vector<int> radices;
     int LD;

@@ -23,6 +23,7 @@ SkEntry make_entry(std::vector<int> radices) {
     e.mode = K::MODE;
     e.sign = K::SIGN;
     e.tw4 = K::TW4;
+    e.twb = K::TWB;
     e.stages = STAGES;
     e.radices = std::move(radices);
     e.LD = K::LD;
@@ -33,9 +34,9 @@ SkEntry make_entry(std::vector<int> radices) {
 
 template <int SHARD>
 void register_shard(std::vector<SkEntry>& out) {
-#define SIP_SK_ENTRY(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, ...)                                  \
-    if constexpr (S == SHARD) {                                                                              \
-        out.push_back(make_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, __VA_ARGS__>, STAGES>({__VA_ARGS__})); \
+#define SIP_SK_ENTRY(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, ...)                                  \
+    if constexpr (S == SHARD) {                                                                                   \
+        out.push_back(make_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, TWB, __VA_ARGS__>, STAGES>({__VA_ARGS__})); \
     }
     SIP_SK_CONFIGS(SIP_SK_ENTRY)
 #undef SIP_SK_ENTRY

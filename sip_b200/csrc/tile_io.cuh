@@ -35,6 +35,10 @@ enum TileOp : int {
     OP_C2R_HALF = 2,
     OP_R2C_PAIR = 3,
     OP_C2R_PAIR = 4,
+    // Large real lengths (half length M = n_other x N beyond one tile), fused
+    // into the four-step passes with mirrored tiles (size-specialized only):
+    OP_R2C_4B = 5,  // pass B: rows k1 and N1-k1 of Y, R2C post-process -> X
+    OP_C2R_4A = 6,  // pass A: columns n2 and N2-n2 of X, C2R pre-process, column FFT, cross twiddle -> Y
 };
 
 enum TileFlags : int {
@@ -59,6 +63,8 @@ struct TileArgs {
     int ntiles;
     int rows;                // real rows (pair ops)
     int flags;
+    int tw4_shift;           // four-step cross twiddles: split base B = 2^tw4_shift
+    int n_other;             // OP_R2C_4B: rows N1 of Y; OP_C2R_4A: columns N2 of X
     float scale;
     FastDiv div_n;           // / N
     FastDiv div_p;           // / P
@@ -136,13 +142,24 @@ SIP_HD void load_c2c(int tid, int T, const TileArgs& a, const TileCtx& c, float2
     }
 }
 
+// Four-step cross twiddle W_N^m from the split table a.tw2:
+// [W_N^lo for lo < B][W_N^{hi B} for hi < ceil(N/B)], B = 2^tw4_shift,
+// m = hi B + lo.  Both halves are a few KB and stay in L1; the product of two
+// correctly rounded values is within about one ulp.
+SIP_HD float2 cross_tw(const TileArgs& a, long long m) {
+    const long long B = 1LL << a.tw4_shift;
+    const float2 lo = SIP_LDG(a.tw2 + (m & (B - 1)));
+    const float2 hi = SIP_LDG(a.tw2 + B + (m >> a.tw4_shift));
+    return c_mul(lo, hi);
+}
+
 // ------------------------------------------------------------ C2C store
-// TW4: multiply element k of transform p by W_{tw_n}^{(i0 + p) k} (the
-// four-step cross twiddle, table a.tw2 of forward values).
+// TW4: multiply element k of transform p by W_N^{(i0 + p) k} (the four-step
+// cross twiddle).
 template <int SIGN, bool TW4>
 SIP_HD float2 c2c_out_value(const TileArgs& a, const TileCtx& c, const float2* sm, int p, int n) {
     float2 v = sm[p * a.LD + sidx(n)];
-    if (TW4) v = c_tw<SIGN>(v, SIP_LDG(a.tw2 + (long long)(c.i0 + p) * n));
+    if (TW4) v = c_tw<SIGN>(v, cross_tw(a, (long long)(c.i0 + p) * n));
     if (a.flags & TF_SCALE) v = c_scale(v, a.scale);
     return maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
 }

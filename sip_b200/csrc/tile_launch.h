@@ -46,6 +46,9 @@ cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries,
 int basis_entries(const PlanDev& plan);
 cudaError_t gen_basis_twiddles(float2* out, const PlanDev& plan, cudaStream_t stream);
 
+// Split cross-twiddle table of four-step passes (tile_io.cuh cross_tw).
+cudaError_t gen_split_twiddles(float2* out, long long n, int shift, cudaStream_t stream);
+
 // out[k] = exp(-2 pi i k / n), k in [0, count).
 cudaError_t gen_root_twiddles(float2* out, long long n, long long count, cudaStream_t stream);
 

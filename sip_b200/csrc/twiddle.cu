@@ -67,7 +67,22 @@ __global__ void k_root_tw(float2* out, long long n, long long count) {
         out[i] = root_fwd(i, n);
 }
 
+// Split cross-twiddle table: [W_n^lo, lo < B][W_n^{hi B}, hi < ceil(n/B)].
+__global__ void k_split_tw(float2* out, long long n, long long B, long long count) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = root_fwd(i < B ? i : (i - B) * B, n);
+}
+
 }  // namespace
+
+cudaError_t gen_split_twiddles(float2* out, long long n, int shift, cudaStream_t stream) {
+    const long long B = 1LL << shift;
+    const long long count = B + (n + B - 1) / B;
+    const int block = 256;
+    k_split_tw<<<(unsigned)((count + block - 1) / block), block, 0, stream>>>(out, n, B, count);
+    return cudaGetLastError();
+}
 
 cudaError_t gen_stockham_twiddles(float2* out, const PlanDev& plan, int entries, cudaStream_t stream) {
     if (entries <= 0) return cudaSuccess;

@@ -47,6 +47,19 @@ std::vector<float2> stockham_host(const PlanDev& pd) {
     return t;
 }
 
+// Second table of a step: roots W_n^k (kind 1) or the split cross-twiddle
+// table of four-step passes (kind 2, tile_io.cuh cross_tw).
+std::vector<float2> tw2_host(const Step& st) {
+    std::vector<float2> t;
+    if (st.tw2_kind == 1) {
+        for (long long k = 0; k < st.tw2_count; ++k) t.push_back(root_host(k, st.tw2_n));
+    } else if (st.tw2_kind == 2) {
+        const long long B = 1LL << st.L.args.tw4_shift;
+        for (long long k = 0; k < st.tw2_count; ++k) t.push_back(root_host(k < B ? k : (k - B) * B, st.tw2_n));
+    }
+    return t;
+}
+
 // Basis twiddle table of the size-specialized kernels (fft_core.cuh basis_split).
 std::vector<float2> basis_host(const std::vector<int>& radices) {
     std::vector<float2> t;
@@ -94,7 +107,7 @@ template <class K, int PASS>
 void emu_sk_passes(const TileArgs& a, const TileCtx& c, float2* buf) {
     using SP = SkPass<K, PASS>;
     std::vector<typename SP::Regs> regs(K::T);
-    for (int tid = 0; tid < K::T; ++tid) SP::read(tid, a, buf, regs[tid]);
+    for (int tid = 0; tid < K::T; ++tid) SP::read(tid, a, c, buf, regs[tid]);
     if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
         for (int tid = 0; tid < K::T; ++tid) SP::write_global(tid, a, c, regs[tid]);
     } else {
@@ -130,6 +143,7 @@ SkEntry emu_entry(std::vector<int> radices) {
     e.mode = K::MODE;
     e.sign = K::SIGN;
     e.tw4 = K::TW4;
+    e.twb = K::TWB;
     e.stages = STAGES;
     e.radices = std::move(radices);
     e.LD = K::LD;
@@ -144,8 +158,8 @@ namespace sipfft {
 const std::vector<SkEntry>& sk_registry() {
     static const std::vector<SkEntry> reg = [] {
         std::vector<SkEntry> v;
-#define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, ...) \
-    v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
+#define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, ...) \
+    v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, TWB, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
         SIP_SK_CONFIGS(SIP_EMU_SK)
 #undef SIP_EMU_SK
         return v;
@@ -167,12 +181,8 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
     a.src = src;
     a.dst = dst;
     a.plan = &st.host_plan;
-    std::vector<float2> tw = st.sk ? basis_host(st.radices) : stockham_host(st.host_plan);
-    std::vector<float2> tw2;
-    if (st.tw2_kind == 1) {
-        tw2.resize(st.tw2_count);
-        for (long long k = 0; k < st.tw2_count; ++k) tw2[k] = root_host(k, st.tw2_n);
-    }
+    std::vector<float2> tw = (st.sk && st.sk->twb) ? basis_host(st.radices) : stockham_host(st.host_plan);
+    std::vector<float2> tw2 = tw2_host(st);
     a.tw = tw.data();
     a.tw2 = tw2.empty() ? nullptr : tw2.data();
     if (st.sk != nullptr) {
@@ -221,8 +231,7 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
 }
 
 void emu_real_step(const Step& st, const void* src, void* dst) {
-    std::vector<float2> tw(st.tw2_count);
-    for (long long k = 0; k < st.tw2_count; ++k) tw[k] = root_host(k, st.tw2_n);
+    std::vector<float2> tw = tw2_host(st);
     const RealPassArgs& r = st.real;
     const float2* s = static_cast<const float2*>(src);
     float2* d = static_cast<float2*>(dst);

@@ -101,6 +101,10 @@ def _sk_list(emu):
 def _plan_for_sk(op, mode, sign, tw4, n):
     """(type, direction, sizes, batch) of a plan whose steps include this kernel."""
     d = O.FORWARD if sign < 0 else O.INVERSE
+    if op == 5:  # R2C four-step pass B with the mirrored post-process
+        return O.R2C, O.INVERSE, [2 * (1 << 19)], 3
+    if op == 6:  # C2R pre-process with the mirrored four-step pass A
+        return O.C2R, O.FORWARD, [2 * (1 << 19)], 3
     if mode == 0:  # rows
         if op == 0:
             return O.C2C, d, [n], 37
