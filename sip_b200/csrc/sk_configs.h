@@ -37,11 +37,11 @@
     /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000) */      \
     X(6, 500, 8, 200, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 20)              \
     X(7, 500, 8, 200, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 20)               \
-    X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 0, 25, 15, 8)          \
-    X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 0, 25, 15, 8)           \
+    X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 15, 8)          \
+    X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 15, 8)           \
     /* odd real length 2187 = 3^7, two rows per complex FFT */                \
-    X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 0, 27, 9, 9)           \
-    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 0, 27, 9, 9)        \
+    X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 1, 27, 9, 9)           \
+    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)        \
     /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A */      \
     X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)      \
     X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)

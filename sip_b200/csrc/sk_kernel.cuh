@@ -97,6 +97,17 @@ struct SkCfg {
     static_assert(!(TW4 && OP != OP_C2C), "cross twiddles are C2C only");
 };
 
+// Column index of slot q of a C2R_4A tile (-1 when the slot is unused).
+template <class K>
+SIP_HD int sk_c2r4a_col(const TileArgs& a, int i0, int cnt, int q) {
+    const int qq = q < K::H ? q : q - K::H;
+    if (qq >= cnt) return -1;
+    const int col0 = i0 + qq;
+    if (q < K::H) return col0;
+    if (col0 == 0 || 2 * col0 == a.n_other) return -1;
+    return a.n_other - col0;
+}
+
 // ------------------------------------------------------------ staging
 // Copies the tile's input into `stage` (byte-exact image of the input
 // layout: rows [q][n] for the row modes, [n][q] for SK_COLS).
@@ -175,28 +186,25 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
 #endif
         }
     } else if constexpr (K::OP == OP_C2R_4A) {
-        // element n1 of columns n2 = i0 + q (slot q) and N2 - n2 (slot H + q)
+        // element n1 of columns n2 = i0 + q (slot q) and N2 - n2 (slot H + q);
+        // each thread keeps one slot and walks the rows
+        static_assert(T % K::P == 0, "C2R_4A staging maps threads to slots");
         const int n2c = a.n_other;
         const char* xbase = src + (c.in_base - c.i0) * 8;  // X[0] of this batch row
-        for (int e = tid; e < K::N * K::P; e += T) {
-            const int n1 = e / K::P;
-            const int slot = e - n1 * K::P;
-            const int q = slot < K::H ? slot : slot - K::H;
-            const int col0 = c.i0 + q;
-            if (q >= c.cnt) continue;
-            int col = col0;
-            if (slot >= K::H) {
-                if (col0 == 0 || 2 * col0 == n2c) continue;
-                col = n2c - col0;
-            }
-            const char* s = xbase + ((long long)n1 * n2c + col) * 8;
-            char* d = reinterpret_cast<char*>(stage) + (n1 * K::P + slot) * 8;
+        const int slot = tid % K::P;
+        const int col = sk_c2r4a_col<K>(a, c.i0, c.cnt, slot);
+        if (col >= 0) {
+            const char* s = xbase + (long long)col * 8;
+            char* d = reinterpret_cast<char*>(stage) + slot * 8;
+            for (int n1 = tid / K::P; n1 < K::N; n1 += T / K::P) {
 #if defined(__CUDA_ARCH__)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(d)),
-                         "l"(s));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                                 (unsigned)__cvta_generic_to_shared(d + n1 * K::P * 8)),
+                             "l"(s + (long long)n1 * n2c * 8));
 #else
-            for (int b = 0; b < 8; ++b) d[b] = s[b];
+                for (int b = 0; b < 8; ++b) d[n1 * K::P * 8 + b] = s[(long long)n1 * n2c * 8 + b];
 #endif
+            }
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
         const int r0 = 2 * c.i0;
@@ -228,17 +236,6 @@ SIP_HD void sk_zero_missing(int tid, const TileArgs& a, const TileCtx& c, float2
             }
         }
     }
-}
-
-// Column index of slot q of a C2R_4A tile (-1 when the slot is unused).
-template <class K>
-SIP_HD int sk_c2r4a_col(const TileArgs& a, int i0, int cnt, int q) {
-    const int qq = q < K::H ? q : q - K::H;
-    if (qq >= cnt) return -1;
-    const int col0 = i0 + qq;
-    if (q < K::H) return col0;
-    if (col0 == 0 || 2 * col0 == a.n_other) return -1;
-    return a.n_other - col0;
 }
 
 // C2R_4A pass-0 input: Z[k] = E + i W_{2M}^{+k} D, k = n1 N2 + n2, from X[k]
