@@ -173,6 +173,71 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- precision form
+def precision_form(torch, dev, stream, steps: int, warmup: int) -> dict:
+    """1D C2C N = 65536, batch 4096 (2 GiB): FP32 Stockham four-step vs the
+    tensor-core BF16x3 split form, on two input families: i.i.d. N(0,1) and
+    8 complex sinusoids with amplitudes spanning 60 dB + N(0, 1e-6) noise
+    (seed 20261029 + N).  Rel-L2 and max-bin error against the FP64 oracle
+    on a row sample."""
+    from oracle import oracle as O
+    from sip_b200 import _lib as L
+    from sip_b200.fft import FftHandle, check
+
+    n, batch = 65536, 4096
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + n)
+    fams = {}
+    fams["noise"] = torch.complex(torch.randn((batch, n), generator=g, device=dev),
+                                  torch.randn((batch, n), generator=g, device=dev))
+    t = torch.arange(n, device=dev, dtype=torch.float64)
+    acc = torch.zeros((batch, n), dtype=torch.complex128, device=dev)
+    for i in range(8):
+        f = torch.rand((batch, 1), generator=g, device=dev, dtype=torch.float64) * n
+        ph = torch.rand((batch, 1), generator=g, device=dev, dtype=torch.float64) * 2 * math.pi
+        acc += (10 ** (-3 * i / 7)) * torch.exp(1j * (2 * math.pi * torch.remainder(f * t, n) / n + ph))
+    del t
+    acc += 1e-6 * torch.complex(torch.randn((batch, n), generator=g, device=dev, dtype=torch.float64),
+                                torch.randn((batch, n), generator=g, device=dev, dtype=torch.float64))
+    fams["sinusoids"] = acc.to(torch.complex64)
+    del acc
+    y = torch.empty((batch, n), dtype=torch.complex64, device=dev)
+    rows = torch.tensor([0, 1, 777, 2048, 4095], device=dev)
+    out = {"n": n, "batch": batch}
+    for mode, name in ((L.SIP_FFT_COMPUTE_FP32, "fp32"), (L.SIP_FFT_COMPUTE_TC_SPLIT, "tc_split")):
+        h = FftHandle()
+        check(h.set_compute_mode(mode), "mode")
+        check(h.make_plan_1d(n, L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, batch), "plan")
+        h.bind_workspace(dev)
+        check(h.set_stream(stream), "stream")
+        x = fams["noise"]
+        for _ in range(warmup):
+            check(h.exec_raw(x.data_ptr(), y.data_ptr()), "exec")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            check(h.exec_raw(x.data_ptr(), y.data_ptr()), "exec")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res = {"ms": round(ms, 4), "gflops": round(5 * n * math.log2(n) * batch / (ms * 1e-3) / 1e9, 1),
+               "gbs_algorithmic": round(16 * n * batch / (ms * 1e-3) / 1e9, 1),
+               "kernels": [s["what"] for s in h.describe()["steps"]]}
+        for fam, xf in fams.items():
+            check(h.exec_raw(xf.data_ptr(), y.data_ptr()), "exec")
+            torch.cuda.synchronize()
+            xs = xf.index_select(0, rows).cpu().numpy()
+            ys = y.index_select(0, rows).cpu().numpy()
+            ref = O.fp64(O.C2C, O.FORWARD, xs, [n])
+            res[f"rel_l2_{fam}"] = float(f"{O.rel_l2(ys, ref):.3e}")
+            res[f"max_bin_{fam}"] = float(f"{O.max_bin_err(ys, ref):.3e}")
+        out[name] = res
+        h.destroy()
+    out["tc_speedup"] = round(out["fp32"]["ms"] / out["tc_split"]["ms"], 3)
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args) -> None:
     import torch
@@ -343,6 +408,10 @@ def run_ours(args) -> None:
                "cpu": O.cpu_info()["model"],
                "sample": res["sample"] + " (oracle/stockham.c, the C restatement of the reference's arithmetic)"}
 
+    prec = None
+    if rank == 0 and not args.no_precision:
+        prec = precision_form(torch, dev, stream, steps=5, warmup=2)
+
     if dist:
         dist.barrier()
     if rank == 0:
@@ -363,6 +432,7 @@ def run_ours(args) -> None:
             "parity": parity,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "precision_form": prec,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
         }
@@ -385,6 +455,7 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows for --only (profiling a smaller case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32 vs tensor-core comparison")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")
     ap.add_argument("--ref-seconds", type=float, default=1.5, help="reference arm seconds per size per step")
     args = ap.parse_args()

@@ -23,6 +23,22 @@ AsdSip::AspbStatus sipFftExecRaw(AsdSip::asdFftHandle handle, const void* input,
  * NUL-terminated when cap > 0) and the full length + 1 into *needed. */
 AsdSip::AspbStatus sipFftDescribePlan(AsdSip::asdFftHandle handle, char* buf, size_t cap, size_t* needed);
 
+/* Compute form of the next MakePlan on this handle (call after Create, before
+ * MakePlan):
+ *   SIP_FFT_COMPUTE_FP32     0  FP32 Stockham passes (default; the drop-in path)
+ *   SIP_FFT_COMPUTE_TC_SPLIT 1  passes of length 256 run as two radix-16
+ *                               DFT-matrix GEMM stages on the tensor cores, BF16
+ *                               operands split in three terms (hi + mid + lo),
+ *                               FP32 accumulation; other passes stay FP32.
+ * Returns INVALID_PARAM for an unknown mode or an already planned handle. */
+#define SIP_FFT_COMPUTE_FP32 0
+#define SIP_FFT_COMPUTE_TC_SPLIT 1
+AsdSip::AspbStatus sipFftSetComputeMode(AsdSip::asdFftHandle handle, int mode);
+
+/* Reads and clears the device error word: bit 0 = a tensor-core kernel's
+ * bounded wait ran out (its results are invalid).  0 after a clean run. */
+AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
+
 /* Library version string. */
 const char* sipFftVersion(void);
 

@@ -33,6 +33,10 @@ ASCEND_FFT_INVERSE = 0x11
 ASCEND_FFT_HORIZONTAL = 0x10
 ASCEND_FFT_VERTICAL = 0x11
 
+# Compute forms (include/sip_fft_ext.h).
+SIP_FFT_COMPUTE_FP32 = 0
+SIP_FFT_COMPUTE_TC_SPLIT = 1
+
 # aclDataType / aclFormat (include/acl_tensor.h).
 ACL_FLOAT = 0
 ACL_COMPLEX64 = 16
@@ -44,7 +48,7 @@ EXPORTED = [
     "asdFftExecC2CSeparated", "asdFftExecC2R", "asdFftExecR2C", "asdFftExecIstft", "asdFftDestroy",
     "asdFftMakePlan2D", "asdFftMakePlan3D", "asdFftGetWorkspaceSize", "asdFftSetWorkspace",
     "asdFftSynchronize", "asdFftGetType", "asdFftShift", "asdIfftShift",
-    "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion",
+    "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion", "sipFftSetComputeMode", "sipFftTakeDeviceErrors",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -77,6 +81,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftExecRaw": (_i32, [_vp, _vp, _vp]),
         "sipFftDescribePlan": (_i32, [_vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
         "sipFftVersion": (ctypes.c_char_p, []),
+        "sipFftSetComputeMode": (_i32, [_vp, ctypes.c_int]),
+        "sipFftTakeDeviceErrors": (_i32, [ctypes.POINTER(ctypes.c_uint)]),
         "aclCreateTensor": (_vp, [ctypes.POINTER(_i64), ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_i64), _i64,
                                   ctypes.c_int, ctypes.POINTER(_i64), ctypes.c_uint64, _vp]),
         "aclDestroyTensor": (ctypes.c_int, [_vp]),

@@ -34,6 +34,7 @@ UNITS = [
     ("sk_registry.cu", [], "sk_registry.o"),
     ("tile_kernels.cu", [], "tile_kernels.o"),
     ("twiddle.cu", [], "twiddle.o"),
+    ("tc_kernel.cu", [], "tc_kernel.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),

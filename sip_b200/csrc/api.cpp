@@ -21,6 +21,7 @@
 #include "fft_api.h"
 #include "plan.h"
 #include "sip_fft_ext.h"
+#include "tc_launch.h"
 
 using namespace AsdSip;
 using sipfft::FftPlan;
@@ -449,6 +450,23 @@ AspbStatus sipFftDescribePlan(asdFftHandle handle, char* buf, size_t cap, size_t
         buf[n] = '\0';
     }
     return ACL_SUCCESS;
+}
+
+AspbStatus sipFftSetComputeMode(asdFftHandle handle, int mode) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || p->initialized) return ACL_ERROR_INVALID_PARAM;
+    if (mode != sipfft::kComputeFp32 && mode != sipfft::kComputeTcSplit) return ACL_ERROR_INVALID_PARAM;
+    p->compute_mode = mode;
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftTakeDeviceErrors(unsigned* errors) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (errors == nullptr) return ACL_ERROR_INVALID_PARAM;
+    *errors = 0;
+    if (!device_present()) return ACL_SUCCESS;
+    return sipfft::tc_take_error(errors) == cudaSuccess ? ACL_SUCCESS : ACL_ERROR_INTERNAL_ERROR;
 }
 
 const char* sipFftVersion(void) { return "sip_b200-fft 0.1.0"; }

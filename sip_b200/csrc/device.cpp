@@ -12,6 +12,8 @@
 #include <tuple>
 
 #include "plan.h"
+#include "tc_core.cuh"
+#include "tc_launch.h"
 
 namespace sipfft {
 
@@ -24,7 +26,7 @@ void check(cudaError_t e, const char* what) {
 
 struct TableKey {
     int device;
-    int kind;  // 0 stockham, 1 roots, 2 basis, 3 split cross twiddles
+    int kind;  // 0 stockham, 1 roots, 2 basis, 3 split cross twiddles, 4 tensor-core B operand
     long long a, b;
     std::vector<int> radices;
     bool operator<(const TableKey& o) const {
@@ -82,6 +84,21 @@ BufPtr basis_table(int device, const PlanDev& pd, const std::vector<int>& radice
     return b;
 }
 
+// Split B operand (3 x 2 KB, core-matrix layout) of the DFT-16 stage.
+BufPtr tc_bmat_table(int device, int sign) {
+    TableKey key{device, 4, sign, 0, {}};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    std::vector<uint16_t> host(3 * kTcK * kTcK);
+    tc_make_b(sign, host.data());
+    BufPtr b = alloc_buf(host.size() * sizeof(uint16_t), device);
+    check(cudaMemcpy(b->ptr, host.data(), host.size() * sizeof(uint16_t), cudaMemcpyHostToDevice), "cudaMemcpy");
+    g_tables[key] = b;
+    return b;
+}
+
 BufPtr root_table(int device, long long n, long long count) {
     TableKey key{device, 1, n, count, {}};
     std::lock_guard<std::mutex> lk(g_table_mu);
@@ -116,8 +133,20 @@ void prepare_device(FftPlan& plan) {
     for (Step& st : plan.steps) {
         if (st.tw2_kind == 1) st.tw2 = root_table(device, st.tw2_n, st.tw2_count);
         if (st.tw2_kind == 2) st.tw2 = split_table(device, st.tw2_n, st.L.args.tw4_shift);
-        if (st.kind != StepKind::Tile) {
+        if (st.kind == StepKind::RealPost || st.kind == StepKind::RealPre) {
             st.real.tw = static_cast<const float2*>(st.tw2->ptr);
+            continue;
+        }
+        if (st.kind == StepKind::Tc) {
+            st.tc_bmat = tc_bmat_table(device, st.L.sign);
+            st.tw = root_table(device, 256, 256);
+            st.L.args.tw = static_cast<const float2*>(st.tw->ptr);
+            st.L.args.tw2 = st.tw2 ? static_cast<const float2*>(st.tw2->ptr) : nullptr;
+            st.tc_fn = tc_kernel(st.L.sign, st.L.tw4, st.tc_cols_in, st.tc_cols_out);
+            int per_sm = 1, sms = 1;
+            check(tc_prepare(st.tc_fn, &per_sm), "tc_prepare");
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+            st.L.grid = (int)std::min<long long>(st.L.args.ntiles, (long long)sms * (per_sm > 0 ? per_sm : 1));
             continue;
         }
         st.tw = (st.sk && st.sk->twb) ? basis_table(device, st.host_plan, st.radices)
@@ -158,6 +187,10 @@ void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
         char* dst = resolve(st.dst, st.dst_off);
         if (st.kind == StepKind::Tile) {
             check(tile_launch(st.L, src, dst, stream), "tile kernel launch");
+        } else if (st.kind == StepKind::Tc) {
+            check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
+                            st.L.args.tw, stream),
+                  "tensor-core kernel launch");
         } else {
             RealPassArgs a = st.real;
             a.src = reinterpret_cast<const float2*>(src);

@@ -206,6 +206,29 @@ void try_specialize(Step& st, const AxisIO& io) {
     st.what += " [sk P=" + std::to_string(e->P) + "]";
 }
 
+// Compute mode of the plan being built (build_steps runs under the API lock).
+int g_compute_mode = kComputeFp32;
+
+// Tensor-core form: a C2C step of length 256 runs as two BF16x3 split
+// DFT-16 GEMM stages on tcgen05 (tc_kernel.cu) instead of Stockham passes.
+void try_tensor_core(Step& st, const AxisIO& io) {
+    TileLaunch& L = st.L;
+    TileArgs& a = L.args;
+    if (g_compute_mode != kComputeTcSplit || L.op != OP_C2C || a.N != 256) return;
+    st.kind = StepKind::Tc;
+    st.sk = nullptr;
+    st.tc_cols_in = io.in_idist == 1;
+    st.tc_cols_out = io.out_idist == 1;
+    a.P = 8;
+    a.tiles_per_outer = (int)((io.inner + 7) / 8);
+    a.ntiles = (int)((long long)a.tiles_per_outer * io.outer);
+    a.div_p = make_fastdiv(8);
+    a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+    L.block = 128;
+    L.grid = a.ntiles;
+    st.what += " [tensor-core bf16x3]";
+}
+
 Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const AxisIO& io, int flags, int rows,
                     const std::string& what, bool tw4 = false) {
     Step st;
@@ -251,6 +274,7 @@ Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const Axis
     st.what = what;
     (void)tw_entries;
     if (!std::getenv("SIP_FFT_GENERIC_ONLY")) try_specialize(st, io);
+    try_tensor_core(st, io);
     return st;
 }
 
@@ -545,6 +569,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
 }  // namespace
 
 void build_steps(FftPlan& plan) {
+    g_compute_mode = plan.compute_mode;
     plan.steps.clear();
     plan.workspace_need = 0;
     const long long b = plan.batch;
@@ -630,7 +655,7 @@ std::string describe(const FftPlan& plan) {
         os << (i ? "," : "") << "{\"what\":\"" << st.what << "\",\"kind\":" << (int)st.kind << ",\"src\":\""
            << locs[(int)st.src] << "\",\"dst\":\"" << locs[(int)st.dst] << "\",\"src_off\":" << st.src_off
            << ",\"dst_off\":" << st.dst_off;
-        if (st.kind == StepKind::Tile) {
+        if (st.kind == StepKind::Tile || st.kind == StepKind::Tc) {
             const TileArgs& a = st.L.args;
             os << ",\"op\":" << st.L.op << ",\"sign\":" << st.L.sign << ",\"e\":" << st.L.e << ",\"n\":" << a.N
                << ",\"P\":" << a.P << ",\"LD\":" << a.LD << ",\"threads\":" << st.L.block << ",\"grid\":" << st.L.grid

@@ -41,7 +41,7 @@ using BufPtr = std::shared_ptr<DeviceBuf>;
 // Operand of a step.
 enum class Loc : int { In = 0, Out = 1, Ws = 2 };
 
-enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2 };
+enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2, Tc = 3 };
 
 struct Step {
     StepKind kind = StepKind::Tile;
@@ -54,6 +54,9 @@ struct Step {
     int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count
     long long tw2_n = 0, tw2_count = 0;
     const SkEntry* sk = nullptr;      // size-specialized kernel, when compiled for this step
+    bool tc_cols_in = false, tc_cols_out = false;  // tensor-core step operand layouts
+    const void* tc_fn = nullptr;
+    BufPtr tc_bmat;
     BufPtr plan_dev, tw, tw2;
     std::string what;                 // human-readable description
 };
@@ -64,6 +67,7 @@ struct FftPlan {
     std::vector<int64_t> sizes;  // transform dims, outermost first
     int64_t batch = 1;
     bool vertical = false;
+    int compute_mode = 0;  // 0: FP32 Stockham, 1: tensor-core BF16x3 split for length-256 passes
     bool initialized = false;
     bool resources_ready = false;
     int device = -1;
@@ -83,6 +87,9 @@ std::vector<int> choose_radices(int n, int e);
 
 // Largest complex length one tile kernel transforms (shared memory bound).
 constexpr int kMaxTileN = 16384;
+
+constexpr int kComputeFp32 = 0;
+constexpr int kComputeTcSplit = 1;
 
 // Builds the steps of a validated plan (host side only).
 void build_steps(FftPlan& plan);

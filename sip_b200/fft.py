@@ -74,6 +74,9 @@ class FftHandle:
         self.workspace = None  # torch tensor owning the bound workspace
 
     # ------------------------------------------------------------ plans
+    def set_compute_mode(self, mode: int) -> int:
+        return self.lib.sipFftSetComputeMode(self.h, mode)
+
     def make_plan_1d(self, n, fft_type, direction, batch, dim_type=L.ASCEND_FFT_HORIZONTAL) -> int:
         return self.lib.asdFftMakePlan1D(self.h, n, fft_type, direction, batch, dim_type)
 

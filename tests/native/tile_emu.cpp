@@ -21,6 +21,7 @@
 #include "real_math.cuh"
 #include "sk_configs.h"
 #include "sk_kernel.cuh"
+#include "tc_core.cuh"
 
 using namespace sipfft;
 
@@ -230,6 +231,53 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
     }
 }
 
+// Tensor-core step: the kernel's phase functions (tc_core.cuh) per thread,
+// with a host GEMM over the same split operand layouts in place of tcgen05.
+template <int SIGN, bool TW4, bool CI, bool CO>
+void emu_tc_tiles(const TileArgs& a) {
+    std::vector<uint16_t> b(3 * kTcK * kTcK);
+    tc_make_b(SIGN, b.data());
+    std::vector<float2> tw256(256);
+    for (int m = 0; m < 256; ++m) tw256[m] = root_host(m, 256);
+    std::vector<float2> tile(kTcP * kTcLD);
+    std::vector<unsigned char> abuf(3 * kTcTermBytes);
+    std::vector<float> d(kTcRows * kTcK);
+    for (int t = 0; t < a.ntiles; ++t) {
+        const TileCtx c = decode_tile(a, t);
+        for (int tid = 0; tid < kTcThreads; ++tid) tc_load_tile<CI>(tid, a, c, tile.data());
+        for (int stage = 0; stage < 2; ++stage) {
+            for (int tid = 0; tid < kTcThreads; ++tid) {
+                float2 x[16];
+                if (stage == 0) tc_gather1(tile.data(), tid, x); else tc_gather2(tile.data(), tid, x);
+                tc_put_row(abuf.data(), tid, x);
+            }
+            tc_gemm_host(abuf.data(), b.data(), d.data());
+            for (int tid = 0; tid < kTcThreads; ++tid) {
+                float r[32];
+                for (int i = 0; i < 32; ++i) r[i] = d[tid * kTcK + i];
+                if (stage == 0) tc_scatter1<SIGN>(tile.data(), tid, r, tw256.data()); else tc_scatter2(tile.data(), tid, r);
+            }
+        }
+        for (int tid = 0; tid < kTcThreads; ++tid) tc_store_tile<SIGN, TW4, CO>(tid, a, c, tile.data());
+    }
+}
+
+void emu_tc_step(const Step& st, const void* src, void* dst) {
+    TileArgs a = st.L.args;
+    a.src = src;
+    a.dst = dst;
+    std::vector<float2> tw2 = tw2_host(st);
+    a.tw2 = tw2.empty() ? nullptr : tw2.data();
+    const bool ci = st.tc_cols_in, co = st.tc_cols_out, t4 = st.L.tw4;
+#define SIP_EMU_TC(S)                                                   \
+    if (t4) emu_tc_tiles<S, true, true, true>(a);                     \
+    else if (ci && co) emu_tc_tiles<S, false, true, true>(a);         \
+    else if (!ci && co) emu_tc_tiles<S, false, false, true>(a);       \
+    else emu_tc_tiles<S, false, false, false>(a);
+    if (st.L.sign < 0) { SIP_EMU_TC(-1) } else { SIP_EMU_TC(1) }
+#undef SIP_EMU_TC
+}
+
 void emu_real_step(const Step& st, const void* src, void* dst) {
     std::vector<float2> tw = tw2_host(st);
     const RealPassArgs& r = st.real;
@@ -254,9 +302,19 @@ extern "C" {
 // it on host buffers.  Returns 0 on success, the planner's status code on
 // a planning failure, -1 on an emulation failure.  `desc` receives the
 // plan description (JSON) when non-null.
+int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in,
+                  void* out, char* desc, size_t desc_cap, int mode);
+
 int emu_exec(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in, void* out,
              char* desc, size_t desc_cap) {
+    return emu_exec_mode(type, direction, ndim, sizes, batch, in, out, desc, desc_cap, 0);
+}
+
+// As emu_exec with a compute mode (0 FP32, 1 tensor-core split).
+int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in,
+                  void* out, char* desc, size_t desc_cap, int mode) {
     FftPlan p;
+    p.compute_mode = mode;
     p.type = static_cast<AsdSip::asdFftType>(type);
     p.direction = static_cast<AsdSip::asdFftDirection>(direction);
     p.sizes.assign(sizes, sizes + ndim);
@@ -279,6 +337,7 @@ int emu_exec(int type, int direction, int ndim, const long long* sizes, long lon
             char* s = resolve(st.src, st.src_off);
             char* d = resolve(st.dst, st.dst_off);
             if (st.kind == StepKind::Tile) emu_tile_step(st, s, d);
+            else if (st.kind == StepKind::Tc) emu_tc_step(st, s, d);
             else emu_real_step(st, s, d);
         }
     } catch (const std::exception&) {
