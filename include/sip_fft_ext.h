@@ -39,6 +39,38 @@ AsdSip::AspbStatus sipFftSetComputeMode(AsdSip::asdFftHandle handle, int mode);
  * bounded wait ran out (its results are invalid).  0 after a clean run. */
 AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 
+/* Planner hints for the next MakePlan on this handle (after Create, before
+ * MakePlan); 0 restores the planner default.  Explicit hints disable the
+ * tune cache (file named by the SIP_FFT_TUNE_CACHE environment variable,
+ * written by sip_b200.autotune).  */
+#define SIP_FFT_HINT_TILE_TRANSFORMS 1  /* transforms per tile */
+#define SIP_FFT_HINT_ELEMS_PER_THREAD 2 /* 16 or 32 */
+#define SIP_FFT_HINT_GENERIC_ONLY 3     /* 1: runtime-radix tile kernels only */
+#define SIP_FFT_HINT_RADIX_ORDER 4      /* 0: descending radices, 1: ascending */
+AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
+
+/* Batched execution: the passes of many planned handles (generic tile
+ * kernels: plan them with SIP_FFT_HINT_GENERIC_ONLY) run in one persistent
+ * work-queue launch per pass index, replayed from a captured CUDA graph when
+ * the batch's wave structure repeats.  Add binds the operands; Exec enqueues
+ * on `stream` (cudaStream_t); Clear empties the batch for reuse.  Exec runs
+ * on a non-null stream.  SetGate makes the launch wait for *device_flag != 0
+ * (at most poll_limit <= 2^24 polls per CTA, then bit 1 of the status word is
+ * set and the launch does no work); TakeStatus reads and clears the status
+ * word.  Only plans whose passes are all tile passes are accepted (C2C of any
+ * length, real transforms up to one tile per row); others give
+ * ACL_ERROR_API_NOT_SUPPORT.  None of these has a counterpart in the
+ * reference. */
+typedef void* sipFftBatch;
+AsdSip::AspbStatus sipFftBatchCreate(sipFftBatch* batch);
+AsdSip::AspbStatus sipFftBatchDestroy(sipFftBatch batch);
+AsdSip::AspbStatus sipFftBatchClear(sipFftBatch batch);
+AsdSip::AspbStatus sipFftBatchAdd(sipFftBatch batch, AsdSip::asdFftHandle handle, const void* input, void* output);
+AsdSip::AspbStatus sipFftBatchExec(sipFftBatch batch, void* stream);
+AsdSip::AspbStatus sipFftBatchSetGate(sipFftBatch batch, const unsigned* device_flag, long long poll_limit);
+AsdSip::AspbStatus sipFftBatchUseGraphs(sipFftBatch batch, int enable);
+AsdSip::AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status);
+
 /* Library version string. */
 const char* sipFftVersion(void);
 

@@ -37,6 +37,15 @@ ASCEND_FFT_VERTICAL = 0x11
 SIP_FFT_COMPUTE_FP32 = 0
 SIP_FFT_COMPUTE_TC_SPLIT = 1
 
+# Planner hint keys (include/sip_fft_ext.h).
+SIP_FFT_HINT_TILE_TRANSFORMS = 1
+SIP_FFT_HINT_ELEMS_PER_THREAD = 2
+SIP_FFT_HINT_GENERIC_ONLY = 3
+SIP_FFT_HINT_RADIX_ORDER = 4
+
+# Batch status bits.
+SIP_FFT_BATCH_GATE_TIMEOUT = 2
+
 # aclDataType / aclFormat (include/acl_tensor.h).
 ACL_FLOAT = 0
 ACL_COMPLEX64 = 16
@@ -49,6 +58,8 @@ EXPORTED = [
     "asdFftMakePlan2D", "asdFftMakePlan3D", "asdFftGetWorkspaceSize", "asdFftSetWorkspace",
     "asdFftSynchronize", "asdFftGetType", "asdFftShift", "asdIfftShift",
     "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion", "sipFftSetComputeMode", "sipFftTakeDeviceErrors",
+    "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
+    "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -83,6 +94,15 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftVersion": (ctypes.c_char_p, []),
         "sipFftSetComputeMode": (_i32, [_vp, ctypes.c_int]),
         "sipFftTakeDeviceErrors": (_i32, [ctypes.POINTER(ctypes.c_uint)]),
+        "sipFftSetPlanHint": (_i32, [_vp, ctypes.c_int, ctypes.c_int]),
+        "sipFftBatchCreate": (_i32, [ctypes.POINTER(_vp)]),
+        "sipFftBatchDestroy": (_i32, [_vp]),
+        "sipFftBatchClear": (_i32, [_vp]),
+        "sipFftBatchAdd": (_i32, [_vp, _vp, _vp, _vp]),
+        "sipFftBatchExec": (_i32, [_vp, _vp]),
+        "sipFftBatchSetGate": (_i32, [_vp, _vp, ctypes.c_longlong]),
+        "sipFftBatchUseGraphs": (_i32, [_vp, ctypes.c_int]),
+        "sipFftBatchTakeStatus": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint)]),
         "aclCreateTensor": (_vp, [ctypes.POINTER(_i64), ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_i64), _i64,
                                   ctypes.c_int, ctypes.POINTER(_i64), ctypes.c_uint64, _vp]),
         "aclDestroyTensor": (ctypes.c_int, [_vp]),

@@ -35,6 +35,8 @@ UNITS = [
     ("tile_kernels.cu", [], "tile_kernels.o"),
     ("twiddle.cu", [], "twiddle.o"),
     ("tc_kernel.cu", [], "tc_kernel.o"),
+    ("queue.cu", [], "queue.o"),
+    ("batch.cpp", [], "batch.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),

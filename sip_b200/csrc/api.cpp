@@ -8,6 +8,7 @@
 // asdFftExecV2 :1446, tensor matching :1512-1750, asdFftExecC2C/C2R/R2C
 // :1752-1844).  Every call holds one process-wide mutex, as the reference's
 // fft_mtx does; no exception crosses the ABI.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -21,6 +22,7 @@
 #include "fft_api.h"
 #include "plan.h"
 #include "sip_fft_ext.h"
+#include "queue.h"
 #include "tc_launch.h"
 
 using namespace AsdSip;
@@ -54,6 +56,7 @@ bool device_present() {
 // construction failures as INVALID_PARAM (fft_api.cpp:1181-1187).
 AspbStatus finish_plan(FftPlan& plan) {
     try {
+        if (!plan.hints_explicit) sipfft::apply_tune_cache(plan);
         sipfft::build_steps(plan);
         if (device_present()) sipfft::prepare_device(plan);
     } catch (const std::exception& e) {
@@ -467,6 +470,120 @@ AspbStatus sipFftTakeDeviceErrors(unsigned* errors) {
     *errors = 0;
     if (!device_present()) return ACL_SUCCESS;
     return sipfft::tc_take_error(errors) == cudaSuccess ? ACL_SUCCESS : ACL_ERROR_INTERNAL_ERROR;
+}
+
+AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || p->initialized) return ACL_ERROR_INVALID_PARAM;
+    switch (key) {
+        case SIP_FFT_HINT_TILE_TRANSFORMS:
+            if (value < 0 || value > 4096) return ACL_ERROR_INVALID_PARAM;
+            p->hint_p = value;
+            break;
+        case SIP_FFT_HINT_ELEMS_PER_THREAD:
+            if (value != 0 && value != 16 && value != 32) return ACL_ERROR_INVALID_PARAM;
+            p->hint_e = value;
+            break;
+        case SIP_FFT_HINT_GENERIC_ONLY:
+            if (value != 0 && value != 1) return ACL_ERROR_INVALID_PARAM;
+            p->hint_generic = value;
+            break;
+        case SIP_FFT_HINT_RADIX_ORDER:
+            if (value != 0 && value != 1) return ACL_ERROR_INVALID_PARAM;
+            p->hint_order = value;
+            break;
+        default:
+            return ACL_ERROR_INVALID_PARAM;
+    }
+    p->hints_explicit = true;
+    return ACL_SUCCESS;
+}
+
+// ------------------------------------------------------------------ batch
+// Upper bound of a gate wait (polls per CTA), so a flag that is never set
+// ends the launch within seconds.
+constexpr long long kMaxGatePolls = 1LL << 24;
+
+AspbStatus sipFftBatchCreate(sipFftBatch* batch) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr) return ACL_ERROR_INVALID_PARAM;
+    if (!device_present()) return ACL_ERROR_INTERNAL_ERROR;
+    try {
+        *batch = sipfft::batch_create();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] batch create failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchDestroy(sipFftBatch batch) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr) return ACL_ERROR_INVALID_PARAM;
+    sipfft::batch_destroy(static_cast<sipfft::Batch*>(batch));
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchClear(sipFftBatch batch) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr) return ACL_ERROR_INVALID_PARAM;
+    sipfft::batch_clear(static_cast<sipfft::Batch*>(batch));
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchAdd(sipFftBatch batch, asdFftHandle handle, const void* input, void* output) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (batch == nullptr || p == nullptr || !p->initialized || input == nullptr || output == nullptr)
+        return ACL_ERROR_INVALID_PARAM;
+    if (p->workspace_need > 0 && (p->workspace == nullptr || p->workspace_recorded == 0)) return ACL_ERROR_INVALID_PARAM;
+    try {
+        if (!p->resources_ready) sipfft::prepare_device(*p);
+        if (!sipfft::batch_add(static_cast<sipfft::Batch*>(batch), *p, input, output)) return ACL_ERROR_API_NOT_SUPPORT;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] batch add failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchExec(sipFftBatch batch, void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr || stream == nullptr) return ACL_ERROR_INVALID_PARAM;
+    auto* b = static_cast<sipfft::Batch*>(batch);
+    try {
+        sipfft::batch_exec(b, static_cast<cudaStream_t>(stream));
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] batch exec failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchSetGate(sipFftBatch batch, const unsigned* device_flag, long long poll_limit) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr || poll_limit < 0 || poll_limit > kMaxGatePolls) return ACL_ERROR_INVALID_PARAM;
+    sipfft::batch_set_gate(static_cast<sipfft::Batch*>(batch), device_flag, poll_limit);
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchUseGraphs(sipFftBatch batch, int enable) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr) return ACL_ERROR_INVALID_PARAM;
+    sipfft::batch_use_graphs(static_cast<sipfft::Batch*>(batch), enable != 0);
+    return ACL_SUCCESS;
+}
+
+AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (batch == nullptr || status == nullptr) return ACL_ERROR_INVALID_PARAM;
+    try {
+        *status = sipfft::batch_take_status(static_cast<sipfft::Batch*>(batch));
+    } catch (const std::exception&) {
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
 }
 
 const char* sipFftVersion(void) { return "sip_b200-fft 0.1.0"; }

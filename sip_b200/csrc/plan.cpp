@@ -40,6 +40,13 @@ int64_t FftPlan::elements() const {
     return e;
 }
 
+// Compute mode and hints of the plan being built (build_steps runs under the
+// API lock).
+namespace {
+int g_compute_mode = kComputeFp32;
+int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0;
+}  // namespace
+
 // ------------------------------------------------------------ radices
 namespace {
 
@@ -86,7 +93,8 @@ std::vector<int> choose_radices(int n, int e) {
     };
     auto r = best(n);
     if (r.first >= 1e29) return {-1};
-    std::sort(r.second.begin(), r.second.end(), std::greater<int>());
+    if (g_hint_order == 1) std::sort(r.second.begin(), r.second.end());
+    else std::sort(r.second.begin(), r.second.end(), std::greater<int>());
     return r.second;
 }
 
@@ -136,6 +144,8 @@ struct TileShape {
 TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     TileShape s{};
     s.e = (n > 8192 || (column && n >= 1024)) ? 32 : 16;
+    if (g_hint_e == 16 && n <= 8192) s.e = 16;
+    if (g_hint_e == 32) s.e = 32;
     s.LD = even_ld(std::max(rowlen, 1));
     const long long row_bytes = (long long)s.LD * 8;
     long long maxp_thr = std::max<long long>(1, (long long)kMaxTileThreads * s.e / std::max(n, 1));
@@ -145,6 +155,8 @@ TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     } else {
         p = std::min<long long>(maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes));
     }
+    if (g_hint_p > 0)
+        p = std::min<long long>({(long long)g_hint_p, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
     p = std::max<long long>(1, std::min<long long>(p, transforms));
     s.P = (int)p;
     long long t = ((long long)s.P * n + s.e - 1) / s.e;
@@ -206,15 +218,14 @@ void try_specialize(Step& st, const AxisIO& io) {
     st.what += " [sk P=" + std::to_string(e->P) + "]";
 }
 
-// Compute mode of the plan being built (build_steps runs under the API lock).
-int g_compute_mode = kComputeFp32;
+
 
 // Tensor-core form: a C2C step of length 256 runs as two BF16x3 split
 // DFT-16 GEMM stages on tcgen05 (tc_kernel.cu) instead of Stockham passes.
 void try_tensor_core(Step& st, const AxisIO& io) {
     TileLaunch& L = st.L;
     TileArgs& a = L.args;
-    if (g_compute_mode != kComputeTcSplit || L.op != OP_C2C || a.N != 256) return;
+    if (g_compute_mode != kComputeTcSplit || g_hint_generic || L.op != OP_C2C || a.N != 256) return;
     st.kind = StepKind::Tc;
     st.sk = nullptr;
     st.tc_cols_in = io.in_idist == 1;
@@ -273,7 +284,7 @@ Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const Axis
     L.tw4 = tw4;
     st.what = what;
     (void)tw_entries;
-    if (!std::getenv("SIP_FFT_GENERIC_ONLY")) try_specialize(st, io);
+    if (!std::getenv("SIP_FFT_GENERIC_ONLY") && !g_hint_generic) try_specialize(st, io);
     try_tensor_core(st, io);
     return st;
 }
@@ -466,7 +477,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     const size_t zbytes = (size_t)(rows * m * 8);
     int n1 = 0, n2 = 0;
     const bool split = four_step_split(m, &n1, &n2);
-    const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr;
+    const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr || g_hint_generic;
     if (split && !generic_only) {
         const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1) : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1);
         const SkEntry* eb = r2c ? sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2) : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
@@ -568,8 +579,39 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
 
 }  // namespace
 
+bool apply_tune_cache(FftPlan& plan) {
+    const char* path = std::getenv("SIP_FFT_TUNE_CACHE");
+    if (path == nullptr) return false;
+    FILE* f = std::fopen(path, "r");
+    if (f == nullptr) return false;
+    std::string dims;
+    for (size_t i = 0; i < plan.sizes.size(); ++i) dims += (i ? "x" : "") + std::to_string(plan.sizes[i]);
+    char line[512];
+    bool hit = false;
+    while (std::fgets(line, sizeof(line), f)) {
+        int type = 0, dir = 0, p = 0, e = 0, gen = 0, order = 0;
+        long long batch = 0;
+        char d[256] = {0};
+        if (std::sscanf(line, "%d %d %255s %lld %d %d %d %d", &type, &dir, d, &batch, &p, &e, &gen, &order) != 8)
+            continue;
+        if (type == (int)plan.type && dir == (int)plan.direction && dims == d && batch == plan.batch) {
+            plan.hint_p = p;
+            plan.hint_e = e;
+            plan.hint_generic = gen;
+            plan.hint_order = order;
+            hit = true;  // the last matching line wins
+        }
+    }
+    std::fclose(f);
+    return hit;
+}
+
 void build_steps(FftPlan& plan) {
     g_compute_mode = plan.compute_mode;
+    g_hint_p = plan.hint_p;
+    g_hint_e = plan.hint_e;
+    g_hint_generic = plan.hint_generic;
+    g_hint_order = plan.hint_order;
     plan.steps.clear();
     plan.workspace_need = 0;
     const long long b = plan.batch;

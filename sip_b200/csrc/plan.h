@@ -68,6 +68,12 @@ struct FftPlan {
     int64_t batch = 1;
     bool vertical = false;
     int compute_mode = 0;  // 0: FP32 Stockham, 1: tensor-core BF16x3 split for length-256 passes
+    // Planner hints (sipFftSetPlanHint / the tune cache); 0 = planner default.
+    int hint_p = 0;        // transforms per tile
+    int hint_e = 0;        // elements per thread (16 or 32)
+    int hint_generic = 0;  // 1: generic tile kernels only (no size-specialized / tensor-core)
+    int hint_order = 0;    // radix order: 0 descending, 1 ascending
+    bool hints_explicit = false;
     bool initialized = false;
     bool resources_ready = false;
     int device = -1;
@@ -96,6 +102,23 @@ void build_steps(FftPlan& plan);
 
 // Allocates the plan's device tables on the current device.
 void prepare_device(FftPlan& plan);
+
+// Applies the tune-cache entry for the plan (file named by SIP_FFT_TUNE_CACHE,
+// lines "type direction n0[xn1[xn2]] batch P E generic order"); returns true
+// when an entry matched.
+bool apply_tune_cache(FftPlan& plan);
+
+// Batched queue execution (batch.cpp).
+struct Batch;
+Batch* batch_create();
+void batch_destroy(Batch* b);
+void batch_clear(Batch* b);
+bool batch_add(Batch* b, const FftPlan& p, const void* in, void* out);
+void batch_exec(Batch* b, cudaStream_t stream);
+void batch_set_gate(Batch* b, const unsigned* gate, long long limit);
+void batch_use_graphs(Batch* b, bool on);
+unsigned batch_take_status(Batch* b);
+int batch_last_launches(const Batch* b);
 
 // Launches every step on the plan's stream.
 void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws);

@@ -45,6 +45,8 @@ enum TileFlags : int {
     TF_CONJ_IN = 1,   // conjugate every loaded value (C2R forward = hfft)
     TF_CONJ_OUT = 2,  // conjugate every stored value (R2C inverse)
     TF_SCALE = 4,     // multiply stored values by `scale`
+    TF_MUL = 8,       // multiply stored value k of transform i0 + p by
+                      // mul[(i0 + p) * mul_pitch_p + k * mul_pitch_k] (C2C)
 };
 
 struct TileArgs {
@@ -65,6 +67,8 @@ struct TileArgs {
     int flags;
     int tw4_shift;           // four-step cross twiddles: split base B = 2^tw4_shift
     int n_other;             // OP_R2C_4B: rows N1 of Y; OP_C2R_4A: columns N2 of X
+    const float2* mul;       // TF_MUL spectrum (e.g. a matched filter)
+    long long mul_pitch_p, mul_pitch_k;
     float scale;
     FastDiv div_n;           // / N
     FastDiv div_p;           // / P
@@ -160,6 +164,7 @@ template <int SIGN, bool TW4>
 SIP_HD float2 c2c_out_value(const TileArgs& a, const TileCtx& c, const float2* sm, int p, int n) {
     float2 v = sm[p * a.LD + sidx(n)];
     if (TW4) v = c_tw<SIGN>(v, cross_tw(a, (long long)(c.i0 + p) * n));
+    if (a.flags & TF_MUL) v = c_mul(v, SIP_LDG(a.mul + (long long)(c.i0 + p) * a.mul_pitch_p + (long long)n * a.mul_pitch_k));
     if (a.flags & TF_SCALE) v = c_scale(v, a.scale);
     return maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
 }

@@ -52,41 +52,45 @@ __device__ __forceinline__ void run_passes(int tid, int T, const TileArgs& a) {
     }
 }
 
+// One tile of the generic kernel (also the work unit of the batch queue,
+// queue.cu).  T is the block size; any T >= P N / E works.
+template <int SIGN, int E, int OP, bool TW4>
+__device__ __forceinline__ void tile_body(const TileArgs& a, int tile, int tid, int T) {
+    float2* sm = sip_tile_smem;
+    const TileCtx c = decode_tile(a, tile);
+    if constexpr (OP == OP_C2C) {
+        load_c2c(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_R2C_HALF) {
+        load_r2c_half(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_C2R_HALF) {
+        load_c2r_half(tid, T, a, c, sm);
+        __syncthreads();
+        prep_c2r_half(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_R2C_PAIR) {
+        load_r2c_pair(tid, T, a, c, sm);
+    } else {
+        load_c2r_pair(tid, T, a, c, sm);
+    }
+    __syncthreads();
+    run_passes<SIGN, E>(tid, T, a);
+    if constexpr (OP == OP_C2C) {
+        store_c2c<SIGN, TW4>(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_R2C_HALF) {
+        store_r2c_half(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_C2R_HALF) {
+        store_c2r_half(tid, T, a, c, sm);
+    } else if constexpr (OP == OP_R2C_PAIR) {
+        store_r2c_pair(tid, T, a, c, sm);
+    } else {
+        store_c2r_pair(tid, T, a, c, sm);
+    }
+    __syncthreads();
+}
+
 template <int SIGN, int E, int OP, bool TW4>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) tile_fft_kernel(const TileArgs a) {
-    float2* sm = sip_tile_smem;
-    const int tid = threadIdx.x;
-    const int T = blockDim.x;
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const TileCtx c = decode_tile(a, tile);
-        if constexpr (OP == OP_C2C) {
-            load_c2c(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_R2C_HALF) {
-            load_r2c_half(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_C2R_HALF) {
-            load_c2r_half(tid, T, a, c, sm);
-            __syncthreads();
-            prep_c2r_half(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_R2C_PAIR) {
-            load_r2c_pair(tid, T, a, c, sm);
-        } else {
-            load_c2r_pair(tid, T, a, c, sm);
-        }
-        __syncthreads();
-        run_passes<SIGN, E>(tid, T, a);
-        if constexpr (OP == OP_C2C) {
-            store_c2c<SIGN, TW4>(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_R2C_HALF) {
-            store_r2c_half(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_C2R_HALF) {
-            store_c2r_half(tid, T, a, c, sm);
-        } else if constexpr (OP == OP_R2C_PAIR) {
-            store_r2c_pair(tid, T, a, c, sm);
-        } else {
-            store_c2r_pair(tid, T, a, c, sm);
-        }
-        __syncthreads();
-    }
+    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x)
+        tile_body<SIGN, E, OP, TW4>(a, tile, threadIdx.x, blockDim.x);
 }
 
 }  // namespace sipfft

@@ -77,6 +77,9 @@ class FftHandle:
     def set_compute_mode(self, mode: int) -> int:
         return self.lib.sipFftSetComputeMode(self.h, mode)
 
+    def set_hint(self, key: int, value: int) -> int:
+        return self.lib.sipFftSetPlanHint(self.h, key, value)
+
     def make_plan_1d(self, n, fft_type, direction, batch, dim_type=L.ASCEND_FFT_HORIZONTAL) -> int:
         return self.lib.asdFftMakePlan1D(self.h, n, fft_type, direction, batch, dim_type)
 
@@ -148,6 +151,54 @@ class FftHandle:
             self.h = None
         self.workspace = None
         return rc
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched execution of many planned handles (sipFftBatch*): pass k of
+    every added plan runs in one persistent work-queue launch, replayed from
+    a captured CUDA graph when the wave structure repeats."""
+
+    def __init__(self, use_graphs: bool = True):
+        self.lib = L.lib()
+        b = ctypes.c_void_p()
+        check(self.lib.sipFftBatchCreate(ctypes.byref(b)), "sipFftBatchCreate")
+        self.b = b
+        check(self.lib.sipFftBatchUseGraphs(self.b, int(use_graphs)), "sipFftBatchUseGraphs")
+
+    def add(self, handle: FftHandle, in_ptr: int, out_ptr: int) -> int:
+        return self.lib.sipFftBatchAdd(self.b, handle.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr))
+
+    def execute(self, stream) -> int:
+        ptr = getattr(stream, "cuda_stream", stream)
+        return self.lib.sipFftBatchExec(self.b, ctypes.c_void_p(ptr) if ptr else None)
+
+    def clear(self) -> int:
+        return self.lib.sipFftBatchClear(self.b)
+
+    def set_gate(self, flag_ptr: int | None, poll_limit: int = 0) -> int:
+        return self.lib.sipFftBatchSetGate(self.b, ctypes.c_void_p(flag_ptr) if flag_ptr else None, poll_limit)
+
+    def take_status(self) -> int:
+        s = ctypes.c_uint(0)
+        check(self.lib.sipFftBatchTakeStatus(self.b, ctypes.byref(s)), "sipFftBatchTakeStatus")
+        return s.value
+
+    def destroy(self) -> None:
+        if self.b is not None:
+            self.lib.sipFftBatchDestroy(self.b)
+            self.b = None
 
     def __enter__(self):
         return self

@@ -263,3 +263,47 @@ def test_plan_trace_env():
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                        env={**os.environ, "ASDSIP_FFT_PLAN_TRACE": "1"})
     assert "ASDSIP_FFT_PLAN" in r.stderr and "c2c rows" in r.stderr
+
+
+def test_plan_hints(sip_lib, handle):
+    H = L
+    assert sip_lib.sipFftSetPlanHint(handle, 99, 1) == INV
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_ELEMS_PER_THREAD, 8) == INV
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_GENERIC_ONLY, 2) == INV
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_GENERIC_ONLY, 1) == OK
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_ELEMS_PER_THREAD, 32) == OK
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_RADIX_ORDER, 1) == OK
+    assert plan1d(sip_lib, handle, 1000, C2C, F, 8) == OK
+    (st,) = describe(sip_lib, handle)["steps"]
+    assert st["sk"] is False and st["e"] == 32 and st["radices"] == sorted(st["radices"])
+    assert sip_lib.sipFftSetPlanHint(handle, H.SIP_FFT_HINT_GENERIC_ONLY, 0) == INV  # already planned
+
+
+def test_generic_hint_large_real_uses_queueable_passes(sip_lib, handle):
+    assert sip_lib.sipFftSetPlanHint(handle, L.SIP_FFT_HINT_GENERIC_ONLY, 1) == OK
+    assert plan1d(sip_lib, handle, 1 << 20, R2C, F, 1) == OK
+    steps = describe(sip_lib, handle)["steps"]
+    assert all(s["sk"] is False for s in steps if s["kind"] == 0)
+
+
+def test_tune_cache_env(tmp_path):
+    cache = tmp_path / "tune.txt"
+    cache.write_text("# type dir dims batch P E generic order\n16 16 4096 64 1 32 1 0\n")
+    code = ("import ctypes,sys,json; sys.path.insert(0, %r); from sip_b200.fft import FftHandle; "
+            "h=FftHandle(); h.make_plan_1d(4096, 0x10, 0x10, 64); s=h.describe()['steps'][0]; "
+            "print(json.dumps([s['sk'], s['e'], s['P']]))" % str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       env={**os.environ, "SIP_FFT_TUNE_CACHE": str(cache)})
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == [False, 32, 1], r.stderr
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=dict(os.environ))
+    assert json.loads(r.stdout.strip().splitlines()[-1])[0] is True
+
+
+def test_batch_api_without_device(sip_lib, handle):
+    b = ctypes.c_void_p()
+    assert sip_lib.sipFftBatchCreate(None) == INV
+    assert sip_lib.sipFftBatchCreate(ctypes.byref(b)) == INTERNAL  # no CUDA device: no fallback
+    assert sip_lib.sipFftBatchExec(None, None) == INV
+    assert sip_lib.sipFftBatchAdd(None, handle, None, None) == INV
+    assert sip_lib.sipFftBatchTakeStatus(None, None) == INV
+    assert sip_lib.sipFftBatchSetGate(None, None, 0) == INV
