@@ -28,7 +28,7 @@ void chk(cudaError_t e, const char* what) {
 }
 
 bool queueable(const Step& st) {
-    return st.kind == StepKind::Tile && st.sk == nullptr &&
+    return st.kind == StepKind::Tile && st.sk == nullptr && st.L.smem_bytes <= kQueueMaxSmem &&
            (st.L.op == OP_C2C || st.L.op == OP_R2C_HALF || st.L.op == OP_C2R_HALF || st.L.op == OP_R2C_PAIR ||
             st.L.op == OP_C2R_PAIR);
 }
@@ -107,7 +107,7 @@ void batch_exec(Batch* b, cudaStream_t stream) {
         for (const QueueItem& it : b->waves[w]) smem = std::max(smem, it.smem);
     }
     smem = (smem + 32767) / 32768 * 32768;  // bucket so graphs are reused
-    smem = std::min(smem, kMaxTileSmem);
+    smem = std::min(smem, kQueueMaxSmem);
     size_t copy = 4096;  // upload size, bucketed to a power of two for the same reason
     while (copy < bytes) copy *= 2;
     if (copy > b->cap) {

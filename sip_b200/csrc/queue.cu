@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1)
 
 cudaError_t queue_prepare(int smem_bytes, int* ctas_per_sm) {
     const void* fn = reinterpret_cast<const void*>(&queue_kernel);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTileSmem);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kQueueMaxSmem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, kMaxTileThreads, (size_t)smem_bytes);
 }

@@ -57,6 +57,10 @@ struct Batch {
 };
 
 
+// Dynamic shared memory a queue launch may use (the kernel also holds a few
+// bytes of static shared memory).
+constexpr int kQueueMaxSmem = kMaxTileSmem - 1024;
+
 // Status word bits.
 constexpr unsigned kQueueGateTimeout = 2u;
 
