@@ -71,6 +71,24 @@ AsdSip::AspbStatus sipFftBatchSetGate(sipFftBatch batch, const unsigned* device_
 AsdSip::AspbStatus sipFftBatchUseGraphs(sipFftBatch batch, int enable);
 AsdSip::AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status);
 
+/* Runs a planned C2C handle (FP32 compute form) with the same kernels as
+ * the ordinary exec but allocates nothing: the intermediate of two-pass
+ * (four-step) plans goes to a static device array of the library, 32 MiB on
+ * every GPU that loads it, instead of the bound workspace, which is not
+ * needed.  It is for callers that cannot allocate device memory while they
+ * run, such as a real-time signal chain where cudaMalloc/cudaFree would
+ * synchronise the device and stall its other streams, or a host whose GPU
+ * memory belongs to another pool or a fixed budget.  A plan whose workspace
+ * would exceed 32 MiB (batch x length > 4,194,304 complex points for a
+ * two-pass length) gives ACL_ERROR_INVALID_PARAM with a message; a non-C2C
+ * or tensor-core plan gives ACL_ERROR_API_NOT_SUPPORT.  Runs on the plan's
+ * device and stream.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Every call shares the array, so calls whose kernels overlap on
+ * the GPU race: order them, e.g. on one stream.  No counterpart in the
+ * reference. */
+AsdSip::AspbStatus sipFftExecC2CNoAlloc(AsdSip::asdFftHandle handle, const void* input, void* output);
+
 /* Library version string. */
 const char* sipFftVersion(void);
 

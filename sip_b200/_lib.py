@@ -60,6 +60,7 @@ EXPORTED = [
     "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion", "sipFftSetComputeMode", "sipFftTakeDeviceErrors",
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
+    "sipFftExecC2CNoAlloc",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -103,6 +104,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftBatchSetGate": (_i32, [_vp, _vp, ctypes.c_longlong]),
         "sipFftBatchUseGraphs": (_i32, [_vp, ctypes.c_int]),
         "sipFftBatchTakeStatus": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint)]),
+        "sipFftExecC2CNoAlloc": (_i32, [_vp, _vp, _vp]),
         "aclCreateTensor": (_vp, [ctypes.POINTER(_i64), ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_i64), _i64,
                                   ctypes.c_int, ctypes.POINTER(_i64), ctypes.c_uint64, _vp]),
         "aclDestroyTensor": (ctypes.c_int, [_vp]),

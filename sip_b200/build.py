@@ -37,6 +37,7 @@ UNITS = [
     ("tc_kernel.cu", [], "tc_kernel.o"),
     ("queue.cu", [], "queue.o"),
     ("batch.cpp", [], "batch.o"),
+    ("noalloc.cu", [], "noalloc.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),

@@ -22,6 +22,7 @@
 #include "fft_api.h"
 #include "plan.h"
 #include "sip_fft_ext.h"
+#include "noalloc.h"
 #include "queue.h"
 #include "tc_launch.h"
 
@@ -584,6 +585,40 @@ AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status) {
         return ACL_ERROR_INTERNAL_ERROR;
     }
     return ACL_SUCCESS;
+}
+
+// Runs a planned C2C handle with its scratch in the library's static device
+// array (noalloc.cu) instead of the bound workspace, for callers that must
+// not allocate device memory while they run.  Validation happens before any
+// CUDA call; a plan needing more scratch than the array holds is rejected.
+AspbStatus sipFftExecC2CNoAlloc(asdFftHandle handle, const void* input, void* output) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || !p->initialized || input == nullptr || output == nullptr) return ACL_ERROR_INVALID_PARAM;
+    if (p->type != ASCEND_FFT_C2C || p->compute_mode != sipfft::kComputeFp32) {
+        std::fprintf(stderr, "[sip_b200] no-alloc exec: only FP32 C2C plans are supported\n");
+        return ACL_ERROR_API_NOT_SUPPORT;
+    }
+    if (p->workspace_need > sipfft::kNaScratchBytes) {
+        std::fprintf(stderr,
+                     "[sip_b200] no-alloc exec: the plan needs %zu bytes of scratch; the static scratch holds at "
+                     "most %zu bytes (batch x length <= %zu complex points)\n",
+                     (size_t)p->workspace_need, sipfft::kNaScratchBytes, sipfft::kNaScratchBytes / 8);
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    const char* ib = static_cast<const char*>(input);
+    const char* ob = static_cast<const char*>(output);
+    const size_t isz = operand_bytes(*p, true), osz = operand_bytes(*p, false);
+    if (ib != ob && ib < ob + osz && ob < ib + isz) {
+        std::fprintf(stderr, "[sip_b200] input and output overlap\n");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    if (!device_present() || !p->resources_ready) {
+        std::fprintf(stderr, "[sip_b200] no-alloc exec: the plan has no device tables (no GPU at plan time)\n");
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    DeviceGuard g(p->device);
+    return sipfft::noalloc_exec(*p, input, output) == sipfft::kNaOk ? ACL_SUCCESS : ACL_ERROR_INTERNAL_ERROR;
 }
 
 const char* sipFftVersion(void) { return "sip_b200-fft 0.1.0"; }
