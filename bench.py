@@ -244,10 +244,9 @@ def run_ours(args) -> None:
 
     from sip_b200 import _lib as L
     from sip_b200.fft import FftHandle, check
+    from sip_b200.replicas import max_over_ranks, rank_env, reports
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = None
@@ -309,11 +308,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    total_ms = t_start.elapsed_time(t_end)
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end), dist, dev)
 
     # per-exec durations (ms), averaged over steps
     per = []
@@ -386,11 +381,7 @@ def run_ours(args) -> None:
             e2e_step()
         e1.record(stream)
         torch.cuda.synchronize()
-        e_ms = e0.elapsed_time(e1) / ke
-        if dist:
-            t = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
         assert np.allclose(host_out[0][:2].numpy() / plans[0]["n"], host_in[0][:2].numpy(), atol=1e-5)
         hb = sum(t.numel() * 4 for t in host_in)
         db = sum(t.numel() * 4 for t in host_out)
@@ -414,7 +405,7 @@ def run_ours(args) -> None:
 
     if dist:
         dist.barrier()
-    if rank == 0:
+    if reports(rank):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,

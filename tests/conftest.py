@@ -26,22 +26,9 @@ def sip_lib():
 @pytest.fixture(scope="session")
 def emu():
     """The CPU harness over the kernels' host-device phase functions."""
-    import ctypes
+    from tests.native.build_emu import load
 
-    from tests.native import build_emu
-
-    lib = ctypes.CDLL(str(build_emu.build()))
-    c = ctypes
-    lib.emu_exec.argtypes = [c.c_int, c.c_int, c.c_int, c.POINTER(c.c_longlong), c.c_longlong, c.c_void_p,
-                             c.c_void_p, c.c_char_p, c.c_size_t]
-    lib.emu_exec.restype = c.c_int
-    lib.emu_fastdiv_check.argtypes = [c.c_void_p, c.c_void_p, c.c_longlong]
-    lib.emu_fastdiv_check.restype = c.c_longlong
-    lib.emu_radices.argtypes = [c.c_int, c.c_int, c.c_void_p, c.c_int]
-    lib.emu_radices.restype = c.c_int
-    lib.emu_dft.argtypes = [c.c_int, c.c_int, c.c_void_p]
-    lib.emu_dft.restype = c.c_int
-    return lib
+    return load()
 
 
 @pytest.fixture(scope="session")

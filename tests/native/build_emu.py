@@ -29,5 +29,22 @@ def build() -> Path:
     return LIB
 
 
+def load():
+    """Builds (if stale) and loads the harness with its ctypes signatures."""
+    import ctypes as c
+
+    lib = c.CDLL(str(build()))
+    lib.emu_exec.argtypes = [c.c_int, c.c_int, c.c_int, c.POINTER(c.c_longlong), c.c_longlong, c.c_void_p,
+                             c.c_void_p, c.c_char_p, c.c_size_t]
+    lib.emu_exec.restype = c.c_int
+    lib.emu_fastdiv_check.argtypes = [c.c_void_p, c.c_void_p, c.c_longlong]
+    lib.emu_fastdiv_check.restype = c.c_longlong
+    lib.emu_radices.argtypes = [c.c_int, c.c_int, c.c_void_p, c.c_int]
+    lib.emu_radices.restype = c.c_int
+    lib.emu_dft.argtypes = [c.c_int, c.c_int, c.c_void_p]
+    lib.emu_dft.restype = c.c_int
+    return lib
+
+
 if __name__ == "__main__":
     print(build())
