@@ -49,6 +49,21 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_RADIX_ORDER 4      /* 0: descending radices, 1: ascending */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
 
+/* Pulse compression (matched filtering): plans y = IFFT(FFT(x) * F) for
+ * `batch` complex64 rows of length n, with F the filter spectrum (n complex64
+ * values in device memory, owned by the caller and read at exec time).
+ * Execute with asdFftExecC2C or sipFftExecRaw ((batch, n) in and out).  Up to
+ * n = 16384 the whole chain is one kernel (one HBM read and write); above it,
+ * three passes (forward column pass, fused row FFT-multiply-IFFT pass,
+ * inverse column pass) with a workspace of batch * n * 8 bytes.  Flags:
+ * SIP_FFT_PULSE_CONJ_FILTER multiplies by conj(F) (F = the spectrum of the
+ * transmitted pulse); SIP_FFT_PULSE_SCALE scales by 1/n.  The reference
+ * composes this from asdFftExecC2C and asdMul (include/base_api.h). */
+#define SIP_FFT_PULSE_CONJ_FILTER 1
+#define SIP_FFT_PULSE_SCALE 2
+AsdSip::AspbStatus sipFftMakePlanPulse1D(AsdSip::asdFftHandle handle, int64_t n, int64_t batch, const void* filter,
+                                         int flags);
+
 /* Batched execution: the passes of many planned handles (generic tile
  * kernels: plan them with SIP_FFT_HINT_GENERIC_ONLY) run in one persistent
  * work-queue launch per pass index, replayed from a captured CUDA graph when
@@ -66,6 +81,13 @@ AsdSip::AspbStatus sipFftBatchCreate(sipFftBatch* batch);
 AsdSip::AspbStatus sipFftBatchDestroy(sipFftBatch batch);
 AsdSip::AspbStatus sipFftBatchClear(sipFftBatch batch);
 AsdSip::AspbStatus sipFftBatchAdd(sipFftBatch batch, AsdSip::asdFftHandle handle, const void* input, void* output);
+/* As sipFftBatchAdd for the first `rows` rows of the plan's batch
+ * (1 <= rows <= batch), with the plan's workspace for those rows at
+ * `workspace` (rows * (workspace size / batch) bytes; may be null when the
+ * plan needs none), so one plan of the largest batch serves requests of any
+ * smaller batch, each with its own workspace.  C2C and pulse plans only. */
+AsdSip::AspbStatus sipFftBatchAddRows(sipFftBatch batch, AsdSip::asdFftHandle handle, const void* input, void* output,
+                                      int64_t rows, void* workspace);
 AsdSip::AspbStatus sipFftBatchExec(sipFftBatch batch, void* stream);
 AsdSip::AspbStatus sipFftBatchSetGate(sipFftBatch batch, const unsigned* device_flag, long long poll_limit);
 AsdSip::AspbStatus sipFftBatchUseGraphs(sipFftBatch batch, int enable);

@@ -23,6 +23,10 @@ Pieces (hicann/sip paths relative to the reference root):
   reference's Stockham / real pack arithmetic (oracle/stockham.c), and
   `ref_stockham_c2c` of the reference's own Stockham core compiled for
   the CPU (oracle/_ref, present only where the reference sources were).
+* `chirp_spectrum` / `pulse`: FP64 pulse compression IFFT(FFT(x) * F), the
+  matched-filter chain the reference composes from asdFftExecC2C and asdMul
+  (include/base_api.h:29), with the linear-chirp pulse of the serving
+  workload.
 """
 from __future__ import annotations
 
@@ -140,6 +144,25 @@ def fp64(op: int, direction: int, x: np.ndarray, sizes) -> np.ndarray:
     if direction == FORWARD:
         z = np.conj(z)
     return np.fft.irfftn(z, s=sizes, axes=axes, norm="forward")
+
+
+def chirp_spectrum(n: int) -> np.ndarray:
+    """Spectrum of a linear chirp c[t] = exp(i pi t^2 / L), L = max(1, n // 4),
+    zero-padded to n (the pulse-compression workload's transmitted pulse)."""
+    L = max(1, n // 4)
+    c = np.zeros(n, np.complex128)
+    t = np.arange(L)
+    c[:L] = np.exp(1j * np.pi * t * t / L)
+    return np.fft.fft(c)
+
+
+def pulse(x: np.ndarray, filt: np.ndarray, conj: bool = False, scale: bool = False) -> np.ndarray:
+    """FP64 pulse compression of each row: IFFT(FFT(x) * F), unnormalised
+    (times 1/n with `scale`), F conjugated with `conj` (matched filter)."""
+    n = x.shape[-1]
+    f = np.conj(filt.astype(np.complex128)) if conj else filt.astype(np.complex128)
+    y = np.fft.ifft(np.fft.fft(x.astype(np.complex128), axis=-1) * f, axis=-1)
+    return y if scale else y * n
 
 
 def golden(op: int, direction: int, x: np.ndarray, sizes) -> np.ndarray:

@@ -43,6 +43,10 @@ SIP_FFT_HINT_ELEMS_PER_THREAD = 2
 SIP_FFT_HINT_GENERIC_ONLY = 3
 SIP_FFT_HINT_RADIX_ORDER = 4
 
+# Pulse-compression flags.
+SIP_FFT_PULSE_CONJ_FILTER = 1
+SIP_FFT_PULSE_SCALE = 2
+
 # Batch status bits.
 SIP_FFT_BATCH_GATE_TIMEOUT = 2
 
@@ -60,7 +64,7 @@ EXPORTED = [
     "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion", "sipFftSetComputeMode", "sipFftTakeDeviceErrors",
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
-    "sipFftExecC2CNoAlloc",
+    "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -105,6 +109,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftBatchUseGraphs": (_i32, [_vp, ctypes.c_int]),
         "sipFftBatchTakeStatus": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint)]),
         "sipFftExecC2CNoAlloc": (_i32, [_vp, _vp, _vp]),
+        "sipFftMakePlanPulse1D": (_i32, [_vp, _i64, _i64, _vp, ctypes.c_int]),
+        "sipFftBatchAddRows": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
         "aclCreateTensor": (_vp, [ctypes.POINTER(_i64), ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_i64), _i64,
                                   ctypes.c_int, ctypes.POINTER(_i64), ctypes.c_uint64, _vp]),
         "aclDestroyTensor": (ctypes.c_int, [_vp]),

@@ -549,6 +549,25 @@ AspbStatus sipFftBatchAdd(sipFftBatch batch, asdFftHandle handle, const void* in
     return ACL_SUCCESS;
 }
 
+AspbStatus sipFftBatchAddRows(sipFftBatch batch, asdFftHandle handle, const void* input, void* output, int64_t rows,
+                              void* workspace) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (batch == nullptr || p == nullptr || !p->initialized || input == nullptr || output == nullptr)
+        return ACL_ERROR_INVALID_PARAM;
+    if (rows < 1 || rows > p->batch) return ACL_ERROR_INVALID_PARAM;
+    if (p->workspace_need > 0 && workspace == nullptr) return ACL_ERROR_INVALID_PARAM;
+    try {
+        if (!p->resources_ready) sipfft::prepare_device(*p);
+        if (!sipfft::batch_add_rows(static_cast<sipfft::Batch*>(batch), *p, input, output, rows, workspace))
+            return ACL_ERROR_API_NOT_SUPPORT;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] batch add failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
 AspbStatus sipFftBatchExec(sipFftBatch batch, void* stream) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (batch == nullptr || stream == nullptr) return ACL_ERROR_INVALID_PARAM;
@@ -585,6 +604,24 @@ AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status) {
         return ACL_ERROR_INTERNAL_ERROR;
     }
     return ACL_SUCCESS;
+}
+
+AspbStatus sipFftMakePlanPulse1D(asdFftHandle handle, int64_t fftSize, int64_t batchSize, const void* filter,
+                                 int flags) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || p->initialized || filter == nullptr) return ACL_ERROR_INVALID_PARAM;
+    if (fftSize <= 0 || fftSize > kMaxFftSize) return ACL_ERROR_INVALID_PARAM;
+    if (batchSize <= 0 || batchSize > (int64_t)std::numeric_limits<int32_t>::max()) return ACL_ERROR_INVALID_PARAM;
+    if ((flags & ~(sipfft::kPulseConj | sipfft::kPulseScale)) != 0) return ACL_ERROR_INVALID_PARAM;
+    p->type = ASCEND_FFT_C2C;
+    p->direction = ASCEND_FFT_FORWARD;
+    p->sizes = {fftSize};
+    p->batch = batchSize;
+    p->pulse = true;
+    p->pulse_filter = filter;
+    p->pulse_flags = flags;
+    return finish_plan(*p);
 }
 
 // Runs a planned C2C handle with its scratch in the library's static device

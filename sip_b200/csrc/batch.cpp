@@ -30,7 +30,7 @@ void chk(cudaError_t e, const char* what) {
 bool queueable(const Step& st) {
     return st.kind == StepKind::Tile && st.sk == nullptr && st.L.smem_bytes <= kQueueMaxSmem &&
            (st.L.op == OP_C2C || st.L.op == OP_R2C_HALF || st.L.op == OP_C2R_HALF || st.L.op == OP_R2C_PAIR ||
-            st.L.op == OP_C2R_PAIR);
+            st.L.op == OP_C2R_PAIR || st.L.op == OP_PC);
 }
 
 }  // namespace
@@ -51,18 +51,36 @@ void batch_clear(Batch* b) { b->waves.clear(); }
 // Adds every pass of a planned handle; all passes must be generic tile
 // passes (the planner's generic-only hint gives such plans).
 bool batch_add(Batch* b, const FftPlan& p, const void* in, void* out) {
-    for (const Step& st : p.steps)
+    return batch_add_rows(b, p, in, out, p.batch, p.workspace);
+}
+
+bool batch_add_rows(Batch* b, const FftPlan& p, const void* in, void* out, long long rows, void* ws) {
+    if (rows < 1 || rows > p.batch) return false;
+    for (const Step& st : p.steps) {
         if (!queueable(st)) return false;
+        if (rows != p.batch && st.batch_dim == 0) return false;
+    }
     if ((int)b->waves.size() < (int)p.steps.size()) b->waves.resize(p.steps.size());
     for (size_t k = 0; k < p.steps.size(); ++k) {
         const Step& st = p.steps[k];
         auto loc = [&](Loc l, size_t off) -> char* {
             char* base = l == Loc::In ? const_cast<char*>(static_cast<const char*>(in))
-                       : l == Loc::Out ? static_cast<char*>(out) : static_cast<char*>(p.workspace);
+                       : l == Loc::Out ? static_cast<char*>(out) : static_cast<char*>(ws);
             return base + off;
         };
         QueueItem it{};
         it.args = st.L.args;
+        if (rows != p.batch) {
+            TileArgs& a = it.args;
+            if (st.batch_dim == 1) {
+                a.inner = (int)rows;
+                a.tiles_per_outer = (int)((rows + a.P - 1) / a.P);
+                a.ntiles = a.tiles_per_outer;
+                a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+            } else {
+                a.ntiles = (int)(a.tiles_per_outer * rows);
+            }
+        }
         it.args.src = loc(st.src, st.src_off);
         it.args.dst = loc(st.dst, st.dst_off);
         it.sign = st.L.sign;

@@ -326,6 +326,7 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
         io.out_idist = n;
         Step st = make_tile_step(OP_C2C, sign, (int)n, (int)n, false, io, o.last_flags, 0,
                                  "c2c rows n=" + std::to_string(n));
+        st.batch_dim = 1;
         st.L.args.scale = o.last_scale;
         st.src = o.src;
         st.dst = o.dst;
@@ -377,6 +378,8 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
     Step sb = make_tile_step(OP_C2C, sign, n2, n2, true, b, o.last_flags, 0,
                              "four-step B n=" + std::to_string(n) + " n2=" + std::to_string(n2));
     sb.L.args.scale = o.last_scale;
+    sa.batch_dim = 2;
+    sb.batch_dim = 2;
     sb.src = Loc::Ws;
     sb.src_off = o.scratch_off;
     sb.dst = o.dst;
@@ -384,6 +387,95 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
     plan.steps.push_back(sa);
     plan.steps.push_back(sb);
     plan.workspace_need = std::max(plan.workspace_need, o.scratch_off + (size_t)(batch * n * 8));
+}
+
+// Pulse compression y = IFFT(FFT(x) * F) of every row (length n, batch
+// rows), F the filter spectrum (conjugated with kPulseConj), optionally
+// scaled by 1/n.  Up to one tile the chain is one kernel (OP_PC: load, forward
+// passes, multiply, inverse passes, store).  Above it the four-step
+// factorisation n = n1 n2 is kept open in the middle:
+//   pass A (existing): n1-point FFTs down the columns, times W_n^{n2 k1},
+//          into Y[k1][n2] in the workspace;
+//   pass P (OP_PC, rows of Y in place): n2-point forward FFT giving
+//          X[k1 + n1 k2], times F[k1 + n1 k2], n2-point inverse FFT over k2,
+//          times W_n^{-k1 m2};
+//   pass C: n1-point inverse FFTs down the columns into y[m2 + n2 m1].
+// Three HBM round trips instead of five (forward four-step, multiply,
+// inverse four-step), and no transposed store.
+void add_pulse(FftPlan& plan) {
+    const long long n = plan.sizes[0], batch = plan.batch;
+    const bool cj = (plan.pulse_flags & kPulseConj) != 0;
+    const bool sc = (plan.pulse_flags & kPulseScale) != 0;
+    const auto* filt = static_cast<const float2*>(plan.pulse_filter);
+    const int mul_flags = cj ? TF_MUL_CONJ : 0;
+    const int out_flags = sc ? TF_SCALE : 0;
+    const float scale = 1.0f / (float)n;
+    if (n <= kMaxTileN) {
+        AxisIO io;
+        io.inner = batch;
+        io.in_idist = n;
+        io.out_idist = n;
+        Step st = make_tile_step(OP_PC, 1, (int)n, (int)n, false, io, mul_flags | out_flags, 0,
+                                 "pulse rows n=" + std::to_string(n));
+        st.L.args.mul = filt;
+        st.L.args.mul_pitch_p = 0;
+        st.L.args.mul_pitch_k = 1;
+        st.L.args.scale = scale;
+        st.batch_dim = 1;
+        plan.steps.push_back(st);
+        return;
+    }
+    int n1 = 0, n2 = 0;
+    if (!four_step_split(n, &n1, &n2))
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " has no four-step split");
+    int shift = 0;
+    while ((1LL << (2 * shift)) < n) ++shift;
+    const long long split_count = (1LL << shift) + (n + (1LL << shift) - 1) / (1LL << shift);
+    AxisIO a;  // columns of x viewed as [n1][n2]
+    a.inner = n2;
+    a.outer = batch;
+    a.in_odist = n;
+    a.in_idist = 1;
+    a.in_stride = n2;
+    a.out_odist = n;
+    a.out_idist = 1;
+    a.out_stride = n2;
+    Step sa = make_tile_step(OP_C2C, -1, n1, n1, true, a, 0, 0,
+                             "four-step A n=" + std::to_string(n) + " n1=" + std::to_string(n1), true);
+    sa.L.args.tw4_shift = shift;
+    sa.tw2_kind = 2;
+    sa.tw2_n = n;
+    sa.tw2_count = split_count;
+    sa.src = Loc::In;
+    sa.dst = Loc::Ws;
+    AxisIO r;  // rows of Y, in place
+    r.inner = n1;
+    r.outer = batch;
+    r.in_odist = n;
+    r.in_idist = n2;
+    r.out_odist = n;
+    r.out_idist = n2;
+    Step sp = make_tile_step(OP_PC, 1, n2, n2, false, r, mul_flags, 0,
+                             "pulse rows n=" + std::to_string(n) + " n2=" + std::to_string(n2), true);
+    sp.L.args.tw4_shift = shift;
+    sp.tw2_kind = 2;
+    sp.tw2_n = n;
+    sp.tw2_count = split_count;
+    sp.L.args.mul = filt;
+    sp.L.args.mul_pitch_p = 1;
+    sp.L.args.mul_pitch_k = n1;
+    sp.src = Loc::Ws;
+    sp.dst = Loc::Ws;
+    Step sc3 = make_tile_step(OP_C2C, 1, n1, n1, true, a, out_flags, 0,
+                              "pulse inverse columns n=" + std::to_string(n) + " n1=" + std::to_string(n1));
+    sc3.L.args.scale = scale;
+    sc3.src = Loc::Ws;
+    sc3.dst = Loc::Out;
+    sa.batch_dim = sp.batch_dim = sc3.batch_dim = 2;
+    plan.steps.push_back(sa);
+    plan.steps.push_back(sp);
+    plan.steps.push_back(sc3);
+    plan.workspace_need = (size_t)(batch * n * 8);
 }
 
 // Real transform along contiguous rows of length n (rows rows), one tile.
@@ -614,6 +706,10 @@ void build_steps(FftPlan& plan) {
     g_hint_order = plan.hint_order;
     plan.steps.clear();
     plan.workspace_need = 0;
+    if (plan.pulse) {
+        add_pulse(plan);
+        return;
+    }
     const long long b = plan.batch;
     const auto& sz = plan.sizes;
     const bool c2c = plan.type == ASCEND_FFT_C2C || plan.type == ASCEND_FFT_C2C_SEP;

@@ -49,6 +49,9 @@ struct Step {
     RealPassArgs real{};  // RealPost / RealPre
     Loc src = Loc::In, dst = Loc::Out;
     size_t src_off = 0, dst_off = 0;  // byte offsets into the operand
+    // Which tile index the plan's batch runs along (for executing fewer rows
+    // than planned through the batch queue): 0 neither, 1 inner, 2 outer.
+    int batch_dim = 0;
     PlanDev host_plan{};              // pass list (uploaded to plan_dev)
     std::vector<int> radices;
     int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count
@@ -74,6 +77,11 @@ struct FftPlan {
     int hint_generic = 0;  // 1: generic tile kernels only (no size-specialized / tensor-core)
     int hint_order = 0;    // radix order: 0 descending, 1 ascending
     bool hints_explicit = false;
+    // Pulse-compression plan (sipFftMakePlanPulse1D): x -> IFFT(FFT(x) * F)
+    // per row, F a device spectrum of length sizes[0] owned by the caller.
+    bool pulse = false;
+    const void* pulse_filter = nullptr;
+    int pulse_flags = 0;  // SIP_FFT_PULSE_CONJ_FILTER | SIP_FFT_PULSE_SCALE
     bool initialized = false;
     bool resources_ready = false;
     int device = -1;
@@ -95,6 +103,8 @@ std::vector<int> choose_radices(int n, int e);
 constexpr int kMaxTileN = 16384;
 
 constexpr int kComputeFp32 = 0;
+constexpr int kPulseConj = 1;   // multiply by conj(F)
+constexpr int kPulseScale = 2;  // scale the output by 1/n
 constexpr int kComputeTcSplit = 1;
 
 // Builds the steps of a validated plan (host side only).
@@ -114,6 +124,10 @@ Batch* batch_create();
 void batch_destroy(Batch* b);
 void batch_clear(Batch* b);
 bool batch_add(Batch* b, const FftPlan& p, const void* in, void* out);
+// As batch_add for the first `rows` rows of the plan's batch (rows <= the
+// plan's batch; every step must declare its batch dimension), with the
+// workspace at `ws` (rows * the plan's per-row workspace; null when none).
+bool batch_add_rows(Batch* b, const FftPlan& p, const void* in, void* out, long long rows, void* ws);
 void batch_exec(Batch* b, cudaStream_t stream);
 void batch_set_gate(Batch* b, const unsigned* gate, long long limit);
 void batch_use_graphs(Batch* b, bool on);

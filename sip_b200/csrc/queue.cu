@@ -56,6 +56,13 @@ __device__ void q_dispatch(const QueueItem* it, int tile) {
         case OP_C2R_PAIR:
             if (e32) q_tile<1, 32, OP_C2R_PAIR, false>(a, tile); else q_tile<1, 16, OP_C2R_PAIR, false>(a, tile);
             break;
+        case OP_PC:
+            if (it->tw4) {
+                if (e32) q_tile<1, 32, OP_PC, true>(a, tile); else q_tile<1, 16, OP_PC, true>(a, tile);
+            } else {
+                if (e32) q_tile<1, 32, OP_PC, false>(a, tile); else q_tile<1, 16, OP_PC, false>(a, tile);
+            }
+            break;
         default:
             break;
     }

@@ -41,6 +41,8 @@ KernelFn SIP_INST_NAME(int op, bool tw4) {
             return tile_fft_kernel<S, E, OP_C2R_HALF, false>;
         case OP_C2R_PAIR:
             return tile_fft_kernel<S, E, OP_C2R_PAIR, false>;
+        case OP_PC:  // runs both FFT directions; instantiated once, under sign +1
+            return tw4 ? tile_fft_kernel<S, E, OP_PC, true> : tile_fft_kernel<S, E, OP_PC, false>;
 #endif
         default:
             return nullptr;

@@ -39,6 +39,11 @@ enum TileOp : int {
     // into the four-step passes with mirrored tiles (size-specialized only):
     OP_R2C_4B = 5,  // pass B: rows k1 and N1-k1 of Y, R2C post-process -> X
     OP_C2R_4A = 6,  // pass A: columns n2 and N2-n2 of X, C2R pre-process, column FFT, cross twiddle -> Y
+    // Pulse compression of each tile row in shared memory: forward FFT,
+    // multiply bin k of transform i0 + p by mul[(i0 + p) * mul_pitch_p +
+    // k * mul_pitch_k] (conjugated with TF_MUL_CONJ), inverse FFT, then the
+    // C2C store (cross twiddle with TW4, scaling with TF_SCALE).
+    OP_PC = 7,
 };
 
 enum TileFlags : int {
@@ -47,6 +52,7 @@ enum TileFlags : int {
     TF_SCALE = 4,     // multiply stored values by `scale`
     TF_MUL = 8,       // multiply stored value k of transform i0 + p by
                       // mul[(i0 + p) * mul_pitch_p + k * mul_pitch_k] (C2C)
+    TF_MUL_CONJ = 16, // use conj(mul[...]) (TF_MUL and OP_PC)
 };
 
 struct TileArgs {
@@ -164,7 +170,10 @@ template <int SIGN, bool TW4>
 SIP_HD float2 c2c_out_value(const TileArgs& a, const TileCtx& c, const float2* sm, int p, int n) {
     float2 v = sm[p * a.LD + sidx(n)];
     if (TW4) v = c_tw<SIGN>(v, cross_tw(a, (long long)(c.i0 + p) * n));
-    if (a.flags & TF_MUL) v = c_mul(v, SIP_LDG(a.mul + (long long)(c.i0 + p) * a.mul_pitch_p + (long long)n * a.mul_pitch_k));
+    if (a.flags & TF_MUL) {
+        const float2 m = SIP_LDG(a.mul + (long long)(c.i0 + p) * a.mul_pitch_p + (long long)n * a.mul_pitch_k);
+        v = c_mul(v, maybe_conj(m, (a.flags & TF_MUL_CONJ) != 0));
+    }
     if (a.flags & TF_SCALE) v = c_scale(v, a.scale);
     return maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
 }
@@ -216,6 +225,21 @@ SIP_HD void store_c2c(int tid, int T, const TileArgs& a, const TileCtx& c, const
 }
 
 #undef SIP_C2C_VALUE
+
+// OP_PC: multiplies the spectra held in the tile by the filter spectrum
+// (every element of the tile's transforms, between the two FFTs).
+SIP_HD void mul_tile(int tid, int T, const TileArgs& a, const TileCtx& c, float2* sm) {
+    const int N = a.N;
+    const bool cj = (a.flags & TF_MUL_CONJ) != 0;
+    const int total = c.cnt * N;
+    for (int f = tid; f < total; f += T) {
+        const int p = (int)fd_div(a.div_n, (uint32_t)f);
+        const int n = f - p * N;
+        const float2 m = SIP_LDG(a.mul + (long long)(c.i0 + p) * a.mul_pitch_p + (long long)n * a.mul_pitch_k);
+        float2& v = sm[p * a.LD + sidx(n)];
+        v = c_mul(v, maybe_conj(m, cj));
+    }
+}
 
 // ------------------------------------------------- R2C, even N (half length)
 // Input: rows of 2M reals read as M complex values (row pitch in_idist in

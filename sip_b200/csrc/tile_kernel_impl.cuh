@@ -58,7 +58,7 @@ template <int SIGN, int E, int OP, bool TW4>
 __device__ __forceinline__ void tile_body(const TileArgs& a, int tile, int tid, int T) {
     float2* sm = sip_tile_smem;
     const TileCtx c = decode_tile(a, tile);
-    if constexpr (OP == OP_C2C) {
+    if constexpr (OP == OP_C2C || OP == OP_PC) {
         load_c2c(tid, T, a, c, sm);
     } else if constexpr (OP == OP_R2C_HALF) {
         load_r2c_half(tid, T, a, c, sm);
@@ -72,8 +72,16 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, int tile, int tid, 
         load_c2r_pair(tid, T, a, c, sm);
     }
     __syncthreads();
-    run_passes<SIGN, E>(tid, T, a);
-    if constexpr (OP == OP_C2C) {
+    if constexpr (OP == OP_PC) {
+        // forward FFT, filter, inverse FFT, all in shared memory
+        run_passes<-1, E>(tid, T, a);
+        mul_tile(tid, T, a, c, sm);
+        __syncthreads();
+        run_passes<1, E>(tid, T, a);
+    } else {
+        run_passes<SIGN, E>(tid, T, a);
+    }
+    if constexpr (OP == OP_C2C || OP == OP_PC) {
         store_c2c<SIGN, TW4>(tid, T, a, c, sm);
     } else if constexpr (OP == OP_R2C_HALF) {
         store_r2c_half(tid, T, a, c, sm);

@@ -83,6 +83,11 @@ class FftHandle:
     def make_plan_1d(self, n, fft_type, direction, batch, dim_type=L.ASCEND_FFT_HORIZONTAL) -> int:
         return self.lib.asdFftMakePlan1D(self.h, n, fft_type, direction, batch, dim_type)
 
+    def make_plan_pulse_1d(self, n, batch, filter_ptr: int, flags: int = 0) -> int:
+        """sipFftMakePlanPulse1D: y = IFFT(FFT(x) * F) per row; F lives on the
+        device at filter_ptr (n complex64 values) and must outlive the plan."""
+        return self.lib.sipFftMakePlanPulse1D(self.h, n, batch, ctypes.c_void_p(filter_ptr), flags)
+
     def make_plan_2d(self, x, y, fft_type, direction, batch) -> int:
         return self.lib.asdFftMakePlan2D(self.h, x, y, fft_type, direction, batch)
 
@@ -179,6 +184,10 @@ class Batch:
 
     def add(self, handle: FftHandle, in_ptr: int, out_ptr: int) -> int:
         return self.lib.sipFftBatchAdd(self.b, handle.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr))
+
+    def add_rows(self, handle: FftHandle, in_ptr: int, out_ptr: int, rows: int, ws_ptr: int | None = None) -> int:
+        return self.lib.sipFftBatchAddRows(self.b, handle.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr), rows,
+                                           ctypes.c_void_p(ws_ptr) if ws_ptr else None)
 
     def execute(self, stream) -> int:
         ptr = getattr(stream, "cuda_stream", stream)

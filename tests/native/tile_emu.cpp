@@ -199,7 +199,8 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
         for (auto& v : smv) v = make_float2(nan, nan);
         for (int tid = 0; tid < T; ++tid) {
             switch (st.L.op) {
-                case OP_C2C: load_c2c(tid, T, a, c, sm); break;
+                case OP_C2C:
+                case OP_PC: load_c2c(tid, T, a, c, sm); break;
                 case OP_R2C_HALF: load_r2c_half(tid, T, a, c, sm); break;
                 case OP_C2R_HALF: load_c2r_half(tid, T, a, c, sm); break;
                 case OP_R2C_PAIR: load_r2c_pair(tid, T, a, c, sm); break;
@@ -208,13 +209,18 @@ void emu_tile_step(const Step& st, const void* src, void* dst) {
         }
         if (st.L.op == OP_C2R_HALF)
             for (int tid = 0; tid < T; ++tid) prep_c2r_half(tid, T, a, c, sm);
-        if (st.L.sign < 0) {
+        if (st.L.op == OP_PC) {
+            if (st.L.e == 16) emu_passes<-1, 16>(T, a, sm); else emu_passes<-1, 32>(T, a, sm);
+            for (int tid = 0; tid < T; ++tid) mul_tile(tid, T, a, c, sm);
+            if (st.L.e == 16) emu_passes<1, 16>(T, a, sm); else emu_passes<1, 32>(T, a, sm);
+        } else if (st.L.sign < 0) {
             if (st.L.e == 16) emu_passes<-1, 16>(T, a, sm); else emu_passes<-1, 32>(T, a, sm);
         } else {
             if (st.L.e == 16) emu_passes<1, 16>(T, a, sm); else emu_passes<1, 32>(T, a, sm);
         }
         for (int tid = 0; tid < T; ++tid) {
             switch (st.L.op) {
+                case OP_PC:
                 case OP_C2C:
                     if (st.L.sign < 0) {
                         if (st.L.tw4) store_c2c<-1, true>(tid, T, a, c, sm); else store_c2c<-1, false>(tid, T, a, c, sm);
@@ -305,6 +311,23 @@ extern "C" {
 int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in,
                   void* out, char* desc, size_t desc_cap, int mode);
 
+int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_cap);
+
+// Pulse-compression plan of length n over batch rows with the host filter
+// spectrum `filter` (n complex values) and flags (1 conj, 2 scale 1/n).
+int emu_exec_pulse(long long n, long long batch, const void* filter, int flags, const void* in, void* out,
+                   char* desc, size_t desc_cap) {
+    FftPlan p;
+    p.type = AsdSip::ASCEND_FFT_C2C;
+    p.direction = AsdSip::ASCEND_FFT_FORWARD;
+    p.sizes = {n};
+    p.batch = batch;
+    p.pulse = true;
+    p.pulse_filter = filter;
+    p.pulse_flags = flags;
+    return emu_run_plan(p, in, out, desc, desc_cap);
+}
+
 int emu_exec(int type, int direction, int ndim, const long long* sizes, long long batch, const void* in, void* out,
              char* desc, size_t desc_cap) {
     return emu_exec_mode(type, direction, ndim, sizes, batch, in, out, desc, desc_cap, 0);
@@ -319,6 +342,11 @@ int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, lon
     p.direction = static_cast<AsdSip::asdFftDirection>(direction);
     p.sizes.assign(sizes, sizes + ndim);
     p.batch = batch;
+    return emu_run_plan(p, in, out, desc, desc_cap);
+}
+
+// Builds the plan's steps and runs them on host buffers.
+int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_cap) {
     try {
         build_steps(p);
     } catch (const PlanError& e) {
