@@ -238,6 +238,58 @@ def precision_form(torch, dev, stream, steps: int, warmup: int) -> dict:
     return out
 
 
+def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
+    """Serving form: Poisson pulse-compression requests (N log-uniform over
+    2,3,5-smooth lengths in [256, 2^18], batch uniform 1..512, delayed chirp
+    + N(0, 0.1) noise, matched filter = conj spectrum of the chirp), 16 GB
+    admission budget.  The plain per-request FP32 path (forward C2C,
+    multiply, inverse C2C, LRU(10) plan cache) is first run with every
+    request present at t=0 to measure its capacity; then both paths serve
+    the same arrival sequence at 0.8x and 2x that capacity.  A bounded
+    sample of `count` requests stands in for the 100k-request stream."""
+    from oracle import oracle as O
+    from sip_b200.serve import KIND_PULSE, PlainExecutor, QueueExecutor, Scheduler, make_requests, smooth_lengths
+
+    budget = int(budget_gb * (1 << 30))
+    lengths = smooth_lengths(256, 1 << 18)
+    queue = QueueExecutor(torch, budget, lengths, max_batch=512, streams=3)
+    plain = PlainExecutor(torch, budget, cache_size=10)
+    errs = []
+
+    def check_sample(ex):
+        def cb(group):
+            for r in group:
+                if len(errs) < 12 and r.kind == KIND_PULSE and r.n * r.batch <= (1 << 18):
+                    x = ex.input(r)[:2].cpu().numpy()
+                    y = ex.output(r)[:2].cpu().numpy()
+                    errs.append(O.rel_l2(y, O.pulse(x, O.chirp_spectrum(r.n), conj=True)))
+        return cb
+
+    out = {"requests": count, "budget_gb": budget_gb, "plain_plan_cache": 10,
+           "sample": f"{count} requests of the 100k-request stream (seed 20261203)"}
+    warm = make_requests(64, rate_hz=float("inf"), seed=1)
+    Scheduler(queue, budget).run(warm)
+    Scheduler(plain, budget, max_inflight=64, max_group=1).run(make_requests(64, rate_hz=float("inf"), seed=1))
+    cap = Scheduler(plain, budget, max_inflight=64, max_group=1).run(
+        make_requests(count, rate_hz=float("inf"))).summary()
+    out["plain_capacity"] = cap
+    rate_cap = cap["throughput_req_s"]
+    for f in (0.8, 2.0):
+        rate = f * rate_cap
+        p = Scheduler(plain, budget, max_inflight=64, max_group=1).run(make_requests(count, rate_hz=rate)).summary()
+        q = Scheduler(queue, budget, max_inflight=3, on_complete=check_sample(queue)).run(
+            make_requests(count, rate_hz=rate)).summary()
+        out[f"rate_{f}x"] = {"rate_req_s": round(rate, 1), "plain": p, "queue": q,
+                             "p99_speedup": round(p["p99_ms"] / q["p99_ms"], 3)}
+    out["queue_rel_l2_max"] = float(f"{max(errs):.3e}") if errs else None
+    out["plain_plan_hits"] = plain.hits
+    out["plain_plan_misses"] = plain.misses
+    out["queue_launch_groups"] = queue.launches
+    queue.close()
+    plain.close()
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args) -> None:
     import torch
@@ -402,6 +454,9 @@ def run_ours(args) -> None:
     prec = None
     if rank == 0 and not args.no_precision:
         prec = precision_form(torch, dev, stream, steps=5, warmup=2)
+    serve = None
+    if rank == 0 and not args.no_serve:
+        serve = serving(torch, args.serve_requests)
 
     if dist:
         dist.barrier()
@@ -424,6 +479,7 @@ def run_ours(args) -> None:
             "e2e": e2e,
             "cpu_baseline": cpu,
             "precision_form": prec,
+            "serving": serve,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
         }
@@ -447,6 +503,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 vs tensor-core comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-form comparison")
+    ap.add_argument("--serve-requests", type=int, default=3000, help="requests per serving run")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")
     ap.add_argument("--ref-seconds", type=float, default=1.5, help="reference arm seconds per size per step")
     args = ap.parse_args()

@@ -115,15 +115,19 @@ void batch_exec(Batch* b, cudaStream_t stream) {
     const int nw = (int)b->waves.size();
     b->launches = 0;
     if (nw == 0) return;
-    // layout: [nw headers][wave 0 items][wave 1 items]...
-    size_t bytes = sizeof(QueueWave) * nw;
-    std::vector<size_t> off(nw);
+    // layout: [nw headers][wave 0 items][wave 1 items]...; kernel arguments
+    // depend only on nw, the item offsets travel in the headers
+    const size_t items_off = sizeof(QueueWave) * nw;
+    size_t bytes = items_off;
+    std::vector<int> first(nw);
     int smem = 0;
+    int nitems = 0;
     for (int w = 0; w < nw; ++w) {
-        off[w] = bytes;
-        bytes += sizeof(QueueItem) * std::max<size_t>(1, b->waves[w].size());
+        first[w] = nitems;
+        nitems += (int)b->waves[w].size();
         for (const QueueItem& it : b->waves[w]) smem = std::max(smem, it.smem);
     }
+    bytes += sizeof(QueueItem) * (size_t)std::max(nitems, 1);
     smem = (smem + 32767) / 32768 * 32768;  // bucket so graphs are reused
     smem = std::min(smem, kQueueMaxSmem);
     size_t copy = 4096;  // upload size, bucketed to a power of two for the same reason
@@ -161,9 +165,11 @@ void batch_exec(Batch* b, cudaStream_t stream) {
         }
         hd.items = (int)b->waves[w].size();
         hd.tiles = tiles;
+        hd.first = first[w];
         std::memcpy(h + sizeof(QueueWave) * w, &hd, sizeof(hd));
         if (!b->waves[w].empty())
-            std::memcpy(h + off[w], b->waves[w].data(), sizeof(QueueItem) * b->waves[w].size());
+            std::memcpy(h + items_off + sizeof(QueueItem) * (size_t)first[w], b->waves[w].data(),
+                        sizeof(QueueItem) * b->waves[w].size());
     }
     int per_sm = 1, sms = 1;
     chk(queue_prepare(smem, &per_sm), "queue_prepare");
@@ -174,8 +180,8 @@ void batch_exec(Batch* b, cudaStream_t stream) {
         chk(cudaMemcpyAsync(d, h, copy, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
         for (int w = 0; w < nw; ++w)
             chk(queue_launch(reinterpret_cast<const QueueWave*>(d + sizeof(QueueWave) * w),
-                             reinterpret_cast<const QueueItem*>(d + off[w]), b->counter + w, b->gate, b->gate_limit,
-                             b->status, grid, smem, s),
+                             reinterpret_cast<const QueueItem*>(d + items_off), b->counter + w, b->gate,
+                             b->gate_limit, b->status, grid, smem, s),
                 "queue_launch");
     };
     if (b->use_graphs) {

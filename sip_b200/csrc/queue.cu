@@ -1,8 +1,9 @@
 // Batch work queue: one persistent launch processes the tiles of many
 // transforms of different lengths, batch counts and directions.
 //
-// The host uploads, per wave, a header {items, tiles} followed by the
-// items' QueueItem descriptors (tile arguments + variant + first tile).
+// The host uploads one header {items, tiles, first item} per wave followed
+// by every wave's QueueItem descriptors (tile arguments + variant + first
+// tile).
 // Every CTA repeatedly claims the next tile index with an atomic counter,
 // finds its item by binary search over the items' first tiles and runs the
 // generic tile body (tile_kernel_impl.cuh) of that item's variant.  Items
@@ -69,7 +70,7 @@ __device__ void q_dispatch(const QueueItem* it, int tile) {
 }
 
 __global__ void __launch_bounds__(kMaxTileThreads, 1)
-    queue_kernel(const QueueWave* wave, const QueueItem* items, unsigned* counter, const volatile unsigned* gate,
+    queue_kernel(const QueueWave* wave, const QueueItem* items_base, unsigned* counter, const volatile unsigned* gate,
                  long long gate_limit, unsigned* status) {
     __shared__ int s_tile;
     __shared__ int s_stop;
@@ -85,6 +86,7 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1)
     }
     const int nitems = wave->items;
     const int total = wave->tiles;
+    const QueueItem* items = items_base + wave->first;
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
         __syncthreads();
@@ -110,11 +112,11 @@ cudaError_t queue_prepare(int smem_bytes, int* ctas_per_sm) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, kMaxTileThreads, (size_t)smem_bytes);
 }
 
-cudaError_t queue_launch(const QueueWave* wave, const QueueItem* items, unsigned* counter, const unsigned* gate,
+cudaError_t queue_launch(const QueueWave* wave, const QueueItem* items_base, unsigned* counter, const unsigned* gate,
                          long long gate_limit, unsigned* status, int grid, int smem_bytes, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
-    queue_kernel<<<grid, kMaxTileThreads, smem_bytes, stream>>>(wave, items, counter, gate, gate_limit, status);
+    queue_kernel<<<grid, kMaxTileThreads, smem_bytes, stream>>>(wave, items_base, counter, gate, gate_limit, status);
     return cudaGetLastError();
 }
 

@@ -23,10 +23,14 @@ struct QueueItem {
     int pad_[2];
 };
 
+// Per-wave header: its items are items_base[first .. first + items).  The
+// offsets travel in the uploaded header rather than in kernel arguments, so
+// a captured launch sequence stays valid when the item counts change.
 struct QueueWave {
     int items;
     int tiles;
-    int pad_[2];
+    int first;
+    int pad_;
 };
 
 // Host state of a batch (batch.cpp).
@@ -66,10 +70,10 @@ constexpr unsigned kQueueGateTimeout = 2u;
 
 cudaError_t queue_prepare(int smem_bytes, int* ctas_per_sm);
 
-// Resets the tile counter and launches one wave (header `wave`, `items` in
-// device memory).  `gate` may be null; otherwise CTAs wait (at most
-// gate_limit polls) for *gate != 0.
-cudaError_t queue_launch(const QueueWave* wave, const QueueItem* items, unsigned* counter, const unsigned* gate,
+// Resets the tile counter and launches one wave (header `wave`, items at
+// `items_base` + wave->first, both in device memory).  `gate` may be null;
+// otherwise CTAs wait (at most gate_limit polls) for *gate != 0.
+cudaError_t queue_launch(const QueueWave* wave, const QueueItem* items_base, unsigned* counter, const unsigned* gate,
                          long long gate_limit, unsigned* status, int grid, int smem_bytes, cudaStream_t stream);
 
 }  // namespace sipfft

@@ -79,7 +79,9 @@ struct SkCfg {
                                : (OP == OP_R2C_4B || OP == OP_C2R_4A) ? P * N
                                : OP == OP_C2R_PAIR ? P * (N + 1)
                                : P * N;  // R2C pair: 2P rows of N floats = P*N complex slots
-    static constexpr int BUF = (STAGE > P * LD ? STAGE : P * LD);  // complex values per buffer
+    // Complex values per buffer, rounded up to an even count so that the
+    // second buffer starts on a 16-byte boundary (cp.async 16-byte copies).
+    static constexpr int BUF = ((STAGE > P * LD ? STAGE : P * LD) + 1) / 2 * 2;
     static constexpr int SMEM = 2 * BUF * 8;
     // CTAs per SM the shared memory allows with two stages (228 KB per SM,
     // 1 KB reserved per CTA); used as the register-allocation target.
@@ -113,9 +115,8 @@ SIP_HD int sk_c2r4a_col(const TileArgs& a, int i0, int cnt, int q) {
 // layout: rows [q][n] for the row modes, [n][q] for SK_COLS).
 SIP_HD void sk_copy_run(int tid, int T, float2* stage_base, int stage_off_bytes, const char* src, long long bytes) {
     char* dst = reinterpret_cast<char*>(stage_base) + stage_off_bytes;
-    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-    const int g = ((a | (uintptr_t)bytes | (uintptr_t)stage_off_bytes) & 15) == 0 ? 16
-                : ((a | (uintptr_t)bytes | (uintptr_t)stage_off_bytes) & 7) == 0 ? 8 : 4;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst) | (uintptr_t)bytes;
+    const int g = (a & 15) == 0 ? 16 : (a & 7) == 0 ? 8 : 4;
     const long long chunks = bytes / g;
     for (long long c = tid; c < chunks; c += T) {
 #if defined(__CUDA_ARCH__)
@@ -140,7 +141,8 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
         // [n][q]: one run of cnt adjacent columns per element index n
         const char* base = src + c.in_base * 8;
         const long long pitch = a.in_stride * 8;
-        const uintptr_t align = reinterpret_cast<uintptr_t>(base) | (uintptr_t)pitch | (uintptr_t)(c.cnt * 8);
+        const uintptr_t align = reinterpret_cast<uintptr_t>(base) | (uintptr_t)pitch | (uintptr_t)(c.cnt * 8) |
+                                reinterpret_cast<uintptr_t>(stage) | (uintptr_t)(K::P * 8);
         const int g = (align & 15) == 0 ? 16 : 8;
         const int cpr = c.cnt * 8 / g;  // chunks per run
         const int total = K::N * cpr;
@@ -164,10 +166,13 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
         // rows k1 = i0 + q (slot q) and N1 - k1 (slot H + q) of Y, N values each
         const int n1 = a.n_other;
         const char* ybase = src + (c.in_base - (long long)c.i0 * K::N) * 8;  // row 0 of this batch row
-        constexpr int CPR = K::N * 8 / 16;                                      // 16-byte chunks per row
-        for (int ch = tid; ch < K::P * CPR; ch += T) {
-            const int slot = ch / CPR;
-            const int cc = ch - slot * CPR;
+        // 16-byte copies when the rows are 16-byte aligned (a workspace from
+        // cudaMalloc), 8-byte copies otherwise
+        const int g = ((reinterpret_cast<uintptr_t>(ybase) | reinterpret_cast<uintptr_t>(stage)) & 15) == 0 ? 16 : 8;
+        const int cpr = K::N * 8 / g;  // chunks per row
+        for (int ch = tid; ch < K::P * cpr; ch += T) {
+            const int slot = ch / cpr;
+            const int cc = ch - slot * cpr;
             const int q = slot < K::H ? slot : slot - K::H;
             const int k1 = c.i0 + q;
             if (q >= c.cnt) continue;
@@ -176,13 +181,16 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
                 if (k1 == 0 || 2 * k1 == n1) continue;  // self-mirrored rows
                 row = n1 - k1;
             }
-            const char* s = ybase + (long long)row * K::N * 8 + cc * 16;
-            char* d = reinterpret_cast<char*>(stage) + slot * K::N * 8 + cc * 16;
+            const char* s = ybase + (long long)row * K::N * 8 + cc * g;
+            char* d = reinterpret_cast<char*>(stage) + slot * K::N * 8 + cc * g;
 #if defined(__CUDA_ARCH__)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(d)),
-                         "l"(s));
+            const unsigned da = (unsigned)__cvta_generic_to_shared(d);
+            if (g == 16)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(da), "l"(s));
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(da), "l"(s));
 #else
-            for (int b = 0; b < 16; ++b) d[b] = s[b];
+            for (int b = 0; b < g; ++b) d[b] = s[b];
 #endif
         }
     } else if constexpr (K::OP == OP_C2R_4A) {

@@ -158,3 +158,28 @@ def test_rejects_specialized_plan(cuda):
     with Batch() as bt:
         assert bt.add(h, x.data_ptr(), x.data_ptr()) == L.ACL_ERROR_API_NOT_SUPPORT
     h.destroy()
+
+
+def test_graph_replay_with_changing_item_counts(cuda, jobs):
+    """Replays of one captured graph (same wave count) with different numbers
+    of items per wave: the item offsets travel in the uploaded headers."""
+    from sip_b200.fft import Batch, check
+
+    s = cuda.cuda.Stream()
+    run_batch(cuda, jobs, s)
+    want = {id(j): j.result() for j in jobs}
+    two_pass = [j for j in jobs if len(j.h.describe()["steps"]) == 2]
+    one_pass = [j for j in jobs if len(j.h.describe()["steps"]) == 1]
+    assert two_pass and len(one_pass) >= 3
+    with Batch(True) as bt:
+        for k in range(1, len(one_pass) + 1):
+            bt.clear()
+            sel = one_pass[:k] + two_pass          # wave 0 grows, wave 1 stays
+            for j in sel:
+                j.reset()
+                check(bt.add(j.h, j.xt.data_ptr(), j.yt.data_ptr()), "add")
+            check(bt.execute(s), "exec")
+            s.synchronize()
+            assert bt.take_status() == 0
+            for j in sel:
+                np.testing.assert_array_equal(j.result(), want[id(j)])

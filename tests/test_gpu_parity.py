@@ -77,3 +77,31 @@ def test_known_answers(cuda, pattern, op, n):
             assert np.abs(out).max() == 0
         else:
             assert O.rel_l2(out, g) <= REL_L2_TOL
+
+
+# Every size-specialized kernel with more tiles than resident CTAs, so each
+# CTA transforms several tiles and the double-buffered staging of the next
+# tile runs (grids are capped at SMs x resident CTAs; 148 x 3 = 444 for the
+# smaller kernels).
+@pytest.mark.parametrize("op,direction,n,batch", [
+    (O.C2C, O.FORWARD, 4096, 1000), (O.C2C, O.INVERSE, 4096, 1000),
+    (O.C2C, O.FORWARD, 8192, 700), (O.C2C, O.INVERSE, 8192, 700),
+    (O.C2C, O.FORWARD, 2048, 2000), (O.C2C, O.INVERSE, 1024, 4000),
+    (O.C2C, O.FORWARD, 256, 16000),
+    (O.C2C, O.FORWARD, 65536, 300), (O.C2C, O.INVERSE, 524288, 40),
+    (O.R2C, O.FORWARD, 1000, 8000), (O.C2R, O.INVERSE, 1000, 8000),
+    (O.R2C, O.FORWARD, 6000, 2000), (O.C2R, O.INVERSE, 6000, 2000),
+    (O.R2C, O.FORWARD, 2187, 2001), (O.C2R, O.INVERSE, 2187, 2001),
+    (O.R2C, O.FORWARD, 1 << 20, 12), (O.C2R, O.INVERSE, 1 << 20, 12),
+])
+def test_specialized_kernels_many_tiles_per_cta(cuda, op, direction, n, batch):
+    rng = np.random.default_rng(n + batch)
+    ishape, idt, _, _ = shapes(op, [n], batch)
+    if idt == np.float32:
+        x = rng.uniform(-1, 1, ishape).astype(np.float32)
+    else:
+        x = (rng.standard_normal(ishape) + 1j * rng.standard_normal(ishape)).astype(np.complex64)
+    out = gpu_run(cuda, op, direction, [n], batch, x)
+    rows = np.unique(np.linspace(0, batch - 1, 24).astype(np.int64))
+    err = O.rel_l2(out[rows], O.fp64(op, direction, x[rows], [n]))
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
