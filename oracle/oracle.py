@@ -165,6 +165,22 @@ def pulse(x: np.ndarray, filt: np.ndarray, conj: bool = False, scale: bool = Fal
     return y if scale else y * n
 
 
+def shift2d(x: np.ndarray, row: int, col: int, batch: int, dist: int, inverse: bool, scale: float = 1.0):
+    """Golden of asdFftShift / asdIfftShift (tests/ut/unittest/fft/fftshift/
+    fftshift_data/gen_data.py): each slice s (elements s*dist ..) rolled by
+    ((row+1)//2, (col+1)//2), or by (row//2, col//2) and scaled for the
+    inverse; output slices contiguous."""
+    if dist <= 0:
+        dist = row * col
+    out = np.empty((batch, row, col), np.complex64)
+    sr, sc = (row // 2, col // 2) if inverse else ((row + 1) // 2, (col + 1) // 2)
+    for b in range(batch):
+        sl = x[b * dist:b * dist + row * col].reshape(row, col)
+        r = np.roll(sl, (sr, sc), axis=(0, 1))
+        out[b] = (r * np.float32(scale)).astype(np.complex64) if inverse and scale != 1.0 else r
+    return out
+
+
 def golden(op: int, direction: int, x: np.ndarray, sizes) -> np.ndarray:
     """numpy.fft at the input's precision, cast like the reference's gen_data.py."""
     sizes = tuple(int(s) for s in sizes)

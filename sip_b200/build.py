@@ -38,6 +38,7 @@ UNITS = [
     ("queue.cu", [], "queue.o"),
     ("batch.cpp", [], "batch.o"),
     ("noalloc.cu", [], "noalloc.o"),
+    ("shift.cu", [], "shift.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),

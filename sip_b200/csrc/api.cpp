@@ -24,6 +24,7 @@
 #include "sip_fft_ext.h"
 #include "noalloc.h"
 #include "queue.h"
+#include "shift.h"
 #include "tc_launch.h"
 
 using namespace AsdSip;
@@ -96,6 +97,68 @@ View view_of(const aclTensor* t) {
     if (aclGetDataType(t, &v.dtype) != 0) return v;
     v.ok = true;
     return v;
+}
+
+// Element count of a view, or -1 when a dimension is negative or the product
+// overflows int64.
+int64_t view_elems(const View& v) {
+    int64_t e = 1;
+    for (int64_t d : v.dims) {
+        if (d < 0) return -1;
+        if (d != 0 && e > std::numeric_limits<int64_t>::max() / d) return -1;
+        e *= d;
+    }
+    return e;
+}
+
+// asdFftShift / asdIfftShift with the reference's checks
+// (core/fft/fftshift.cpp:27-140, core/fft/ifftshift.cpp): positive sizes,
+// no int64 overflow, dist <= 0 meaning row * col and 0 < dist < row * col
+// rejected, complex64 tensors holding at least (batch - 1) * dist + row * col
+// input and batch * row * col output elements.  In addition overlapping
+// input and output are rejected (the rotation is not in-place safe) and
+// sizes beyond int32 per axis are not supported.
+AspbStatus run_shift(int64_t row, int64_t col, int64_t batch, int64_t dist, double scale, bool inverse,
+                     const aclTensor* input, aclTensor* output, void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    constexpr int64_t kMax = std::numeric_limits<int64_t>::max();
+    if (row <= 0 || col <= 0 || batch <= 0) return ACL_ERROR_INVALID_PARAM;
+    if (row > kMax / col) return ACL_ERROR_INVALID_PARAM;
+    const int64_t slice = row * col;
+    if (dist <= 0) {
+        dist = slice;
+    } else if (dist < slice) {
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    const View vi = view_of(input), vo = view_of(output);
+    if (!vi.ok || !vo.ok) return ACL_ERROR_INVALID_PARAM;
+    if (vi.dtype != ACL_COMPLEX64 || vo.dtype != ACL_COMPLEX64) return ACL_ERROR_UNSUPPORTED_DATA_TYPE;
+    if (batch - 1 > (kMax - slice) / dist) return ACL_ERROR_INVALID_PARAM;
+    if (batch > kMax / slice) return ACL_ERROR_INVALID_PARAM;
+    const int64_t need_in = (batch - 1) * dist + slice, need_out = batch * slice;
+    const int64_t have_in = view_elems(vi), have_out = view_elems(vo);
+    if (have_in < need_in || have_out < need_out) return ACL_ERROR_INVALID_PARAM;
+    if (row > std::numeric_limits<int32_t>::max() || col > std::numeric_limits<int32_t>::max())
+        return ACL_ERROR_API_NOT_SUPPORT;
+    const char* ib = static_cast<const char*>(aclGetTensorData(input));
+    char* ob = static_cast<char*>(aclGetTensorData(output));
+    if (ib == nullptr || ob == nullptr) return ACL_ERROR_INVALID_PARAM;
+    if (ib < ob + need_out * 8 && ob < ib + need_in * 8) return ACL_ERROR_INVALID_PARAM;
+    if (!device_present()) return ACL_ERROR_INTERNAL_ERROR;
+    sipfft::ShiftArgs a;
+    a.batch = batch;
+    a.dist = dist;
+    a.row = (int)row;
+    a.col = (int)col;
+    a.sr = (int)(inverse ? row / 2 : (row + 1) / 2);
+    a.sc = (int)(inverse ? col / 2 : (col + 1) / 2);
+    a.scale = (float)scale;
+    const cudaError_t e = sipfft::shift_launch(ib, ob, a, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "[sip_b200] shift launch failed: %s\n", cudaGetErrorString(e));
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
 }
 
 // Product of the leading dims [0, count) equals the plan's batch.
@@ -312,12 +375,58 @@ AspbStatus asdFftExecC2C(asdFftHandle handle, const aclTensor* input, const aclT
     return exec_tensors(handle, ASCEND_FFT_C2C, input, output);
 }
 
+// Separated real / imaginary float planes (reference fft_api.cpp:1912-1985):
+// the four views must have equal shapes (else INTERNAL_ERROR) and FLOAT
+// dtype (else OP_INPUT_NOT_MATCH); the trailing dims must equal the plan's
+// sizes and the leading ones its batch (else INVALID_PARAM).
 AspbStatus asdFftExecC2CSeparated(asdFftHandle handle, const aclTensor* inputReal, const aclTensor* inputImag,
                                   const aclTensor* outputReal, const aclTensor* outputImag) {
-    (void)inputReal; (void)inputImag; (void)outputReal; (void)outputImag;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (find_plan(handle) == nullptr) return ACL_ERROR_INVALID_PARAM;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr) return ACL_ERROR_INVALID_PARAM;
+    const View v[4] = {view_of(inputReal), view_of(inputImag), view_of(outputReal), view_of(outputImag)};
+    for (const View& x : v)
+        if (!x.ok) return ACL_ERROR_INVALID_PARAM;
+    for (int i = 1; i < 4; ++i)
+        if (v[i].dims != v[0].dims) return ACL_ERROR_INTERNAL_ERROR;
+    for (const View& x : v)
+        if (x.dtype != ACL_FLOAT) return ACL_ERROR_OP_INPUT_NOT_MATCH;
+    if (!p->initialized) return ACL_ERROR_INVALID_PARAM;
+    if (p->type != ASCEND_FFT_C2C_SEP) return ACL_ERROR_INVALID_PARAM;
+    const auto& d = v[0].dims;
+    if (d.size() < p->sizes.size()) return ACL_ERROR_INVALID_PARAM;
+    const size_t lead = d.size() - p->sizes.size();
+    for (size_t i = 0; i < p->sizes.size(); ++i)
+        if (d[lead + i] != p->sizes[i]) return ACL_ERROR_INVALID_PARAM;
+    if (!leading_is_batch(d, lead, p->batch)) return ACL_ERROR_INVALID_PARAM;
+    const void* ptr[4] = {aclGetTensorData(inputReal), aclGetTensorData(inputImag), aclGetTensorData(outputReal),
+                          aclGetTensorData(outputImag)};
+    for (const void* q : ptr)
+        if (q == nullptr) return ACL_ERROR_INVALID_PARAM;
+    // outputs must not partially overlap the inputs or each other
+    const size_t bytes = (size_t)p->batch * (size_t)p->sizes[0] * 4;
+    auto overlap = [&](const void* a, const void* b) {
+        const char* x = static_cast<const char*>(a);
+        const char* y = static_cast<const char*>(b);
+        return x < y + bytes && y < x + bytes;
+    };
+    if (overlap(ptr[2], ptr[3]) || (overlap(ptr[0], ptr[2]) && ptr[0] != ptr[2]) ||
+        (overlap(ptr[1], ptr[3]) && ptr[1] != ptr[3]) || overlap(ptr[0], ptr[3]) || overlap(ptr[1], ptr[2]))
+        return ACL_ERROR_INVALID_PARAM;
+    try {
+        if (!p->resources_ready) {
+            if (!device_present()) return ACL_ERROR_INTERNAL_ERROR;
+            sipfft::prepare_device(*p);
+        }
+        DeviceGuard g(p->device);
+        sipfft::launch_separated(*p, static_cast<const float*>(ptr[0]), static_cast<const float*>(ptr[1]),
+                                 static_cast<float*>(const_cast<void*>(ptr[2])),
+                                 static_cast<float*>(const_cast<void*>(ptr[3])));
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] separated exec failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
 }
 
 AspbStatus asdFftExecC2R(asdFftHandle handle, const aclTensor* input, const aclTensor* output) {
@@ -422,15 +531,14 @@ AspbStatus asdFftGetType(asdFftHandle handle, asdFftType& fftType) {
 
 AspbStatus asdFftShift(int64_t row, int64_t col, int64_t batch, int64_t dist, const aclTensor* input,
                        aclTensor* output, void* stream, void* workspace) {
-    (void)row; (void)col; (void)batch; (void)dist; (void)input; (void)output; (void)stream; (void)workspace;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    (void)workspace;
+    return run_shift(row, col, batch, dist, 1.0, false, input, output, stream);
 }
 
 AspbStatus asdIfftShift(int64_t row, int64_t col, int64_t batch, int64_t dist, double scale, const aclTensor* input,
                         aclTensor* output, void* stream, void* workspace) {
-    (void)row; (void)col; (void)batch; (void)dist; (void)scale; (void)input; (void)output; (void)stream;
     (void)workspace;
-    return ACL_ERROR_API_NOT_SUPPORT;
+    return run_shift(row, col, batch, dist, scale, true, input, output, stream);
 }
 
 }  // namespace AsdSip

@@ -171,6 +171,16 @@ void prepare_device(FftPlan& plan) {
     plan.resources_ready = true;
 }
 
+void launch_separated(const FftPlan& plan, const float* in_re, const float* in_im, float* out_re, float* out_im) {
+    if (plan.steps.size() != 1 || plan.steps[0].kind != StepKind::Tile || plan.steps[0].sk != nullptr)
+        throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, "separated plan must be one generic tile step");
+    TileLaunch L = plan.steps[0].L;
+    L.args.flags |= TF_PLANAR_IN | TF_PLANAR_OUT;
+    L.args.src_im = in_im;
+    L.args.dst_im = out_im;
+    check(tile_launch(L, in_re, out_re, static_cast<cudaStream_t>(plan.stream)), "tile kernel launch");
+}
+
 void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
     cudaStream_t stream = static_cast<cudaStream_t>(plan.stream);
     auto resolve = [&](Loc l, size_t off) -> char* {

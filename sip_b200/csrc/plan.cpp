@@ -710,6 +710,16 @@ void build_steps(FftPlan& plan) {
         add_pulse(plan);
         return;
     }
+    if (plan.type == ASCEND_FFT_C2C_SEP) {
+        // separated planes: one generic tile pass per transform (the planar
+        // load / store of tile_io.cuh); the reference limits the length to
+        // 2..256, here any one-tile length works
+        if (plan.sizes.size() != 1 || plan.sizes[0] > kMaxTileN)
+            throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "separated C2C supports 1-D lengths up to one tile");
+        g_hint_generic = 1;
+        add_c2c_1d(plan, plan.sizes[0], plan.batch, C2COpts{});
+        return;
+    }
     const long long b = plan.batch;
     const auto& sz = plan.sizes;
     const bool c2c = plan.type == ASCEND_FFT_C2C || plan.type == ASCEND_FFT_C2C_SEP;

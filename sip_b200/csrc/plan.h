@@ -134,6 +134,10 @@ void batch_use_graphs(Batch* b, bool on);
 unsigned batch_take_status(Batch* b);
 int batch_last_launches(const Batch* b);
 
+// Runs a separated-plane C2C plan (one tile step) with real / imaginary
+// float planes.
+void launch_separated(const FftPlan& plan, const float* in_re, const float* in_im, float* out_re, float* out_im);
+
 // Launches every step on the plan's stream.
 void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws);
 

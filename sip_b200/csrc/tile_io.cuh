@@ -53,6 +53,8 @@ enum TileFlags : int {
     TF_MUL = 8,       // multiply stored value k of transform i0 + p by
                       // mul[(i0 + p) * mul_pitch_p + k * mul_pitch_k] (C2C)
     TF_MUL_CONJ = 16, // use conj(mul[...]) (TF_MUL and OP_PC)
+    TF_PLANAR_IN = 32,   // C2C input as two float planes: src (real), src_im (imaginary)
+    TF_PLANAR_OUT = 64,  // C2C output as two float planes: dst (real), dst_im (imaginary)
 };
 
 struct TileArgs {
@@ -74,6 +76,8 @@ struct TileArgs {
     int tw4_shift;           // four-step cross twiddles: split base B = 2^tw4_shift
     int n_other;             // OP_R2C_4B: rows N1 of Y; OP_C2R_4A: columns N2 of X
     const float2* mul;       // TF_MUL spectrum (e.g. a matched filter)
+    const float* src_im;     // TF_PLANAR_IN imaginary plane
+    float* dst_im;           // TF_PLANAR_OUT imaginary plane
     long long mul_pitch_p, mul_pitch_k;
     float scale;
     FastDiv div_n;           // / N
@@ -103,6 +107,18 @@ SIP_HD float2 maybe_conj(float2 v, bool cj) { return cj ? make_float2(v.x, -v.y)
 
 // ------------------------------------------------------------- C2C load
 SIP_HD void load_c2c(int tid, int T, const TileArgs& a, const TileCtx& c, float2* sm) {
+    if (a.flags & TF_PLANAR_IN) {
+        // separated real / imaginary planes (asdFftExecC2CSeparated)
+        const float* re = static_cast<const float*>(a.src);
+        const int total = c.cnt * a.N;
+        for (int f = tid; f < total; f += T) {
+            const int p = (int)fd_div(a.div_n, (uint32_t)f);
+            const int n = f - p * a.N;
+            const long long i = c.in_base + (long long)p * a.in_idist + (long long)n * a.in_stride;
+            sm[p * a.LD + sidx(n)] = make_float2(SIP_LDG(re + i), SIP_LDG(a.src_im + i));
+        }
+        return;
+    }
     const float2* src = static_cast<const float2*>(a.src);
     const int N = a.N, P = a.P, LD = a.LD;
     const bool cj = (a.flags & TF_CONJ_IN) != 0;
@@ -183,6 +199,19 @@ SIP_HD void store_c2c(int tid, int T, const TileArgs& a, const TileCtx& c, const
     float2* dst = static_cast<float2*>(a.dst);
     const int N = a.N, P = a.P;
 #define SIP_C2C_VALUE(p_, n_) c2c_out_value<SIGN, TW4>(a, c, sm, (p_), (n_))
+    if (a.flags & TF_PLANAR_OUT) {
+        float* re = static_cast<float*>(a.dst);
+        const int total = c.cnt * N;
+        for (int f = tid; f < total; f += T) {
+            const int p = (int)fd_div(a.div_n, (uint32_t)f);
+            const int n = f - p * N;
+            const long long i = c.out_base + (long long)p * a.out_idist + (long long)n * a.out_stride;
+            const float2 v = SIP_C2C_VALUE(p, n);
+            re[i] = v.x;
+            a.dst_im[i] = v.y;
+        }
+        return;
+    }
     if (a.out_stride == 1 && a.out_idist == N) {
         float2* base = dst + c.out_base;
         const int count = c.cnt * N;

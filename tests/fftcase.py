@@ -52,6 +52,15 @@ def make_plan(h, op: int, direction: int, sizes, batch: int) -> int:
     return h.make_plan_3d(sizes[0], sizes[1], sizes[2], op, direction, batch)
 
 
+def settle() -> None:
+    """Waits for all work on the device.  The library runs on its own
+    (non-default) stream, so inputs and outputs that torch filled on the
+    default stream must be complete before a test launches on it."""
+    import torch
+
+    torch.cuda.synchronize()
+
+
 def gpu_run(torch, op: int, direction: int, sizes, batch: int, x: np.ndarray, stream=None, keep=False):
     """Plan -> workspace -> stream -> exec through aclTensors -> sync -> destroy."""
     from sip_b200.fft import FftHandle, check
@@ -66,6 +75,7 @@ def gpu_run(torch, op: int, direction: int, sizes, batch: int, x: np.ndarray, st
     s = stream or torch.cuda.Stream()
     check(h.set_stream(s), "set stream")
     fn = {O.C2C: h.exec_c2c, O.R2C: h.exec_r2c, O.C2R: h.exec_c2r}[op]
+    settle()
     check(fn(xt, yt), "exec")
     check(h.synchronize(), "synchronize")
     out = yt.cpu().numpy()

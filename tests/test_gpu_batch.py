@@ -10,7 +10,7 @@ import pytest
 
 from oracle import oracle as O
 from sip_b200 import _lib as L
-from tests.fftcase import make_plan, random_input, shapes
+from tests.fftcase import settle, make_plan, random_input, shapes
 
 pytestmark = pytest.mark.gpu
 
@@ -57,6 +57,7 @@ def run_batch(torch, jobs, stream, use_graphs=True):
     with Batch(use_graphs) as bt:
         for j in jobs:
             check(bt.add(j.h, j.xt.data_ptr(), j.yt.data_ptr()), "batch add")
+        settle()
         check(bt.execute(stream), "batch exec")
         stream.synchronize()
         assert bt.take_status() == 0
@@ -90,6 +91,7 @@ def test_mix_equals_alone_and_plain(cuda, jobs):
         np.testing.assert_array_equal(alone, m, err_msg=str(j.case))  # same kernel, same bits
         j.reset()
         check(j.h.set_stream(s), "stream")
+        settle()
         check(j.h.exec_raw(j.xt.data_ptr(), j.yt.data_ptr()), "exec")
         s.synchronize()
         plain = j.result()
@@ -110,6 +112,7 @@ def test_graph_replay_with_new_operands(cuda, jobs):
             for j in jobs[:4]:
                 j.reset()
                 check(bt.add(j.h, j.xt.data_ptr(), j.yt.data_ptr()), "add")
+            settle()
             check(bt.execute(s), "exec")
             s.synchronize()
             for j, f in zip(jobs[:4], first):
@@ -138,11 +141,13 @@ def test_gate_timeout_sets_status(cuda, jobs):
     with Batch(False) as bt:
         check(bt.set_gate(flag.data_ptr(), 2000), "gate")
         check(bt.add(j.h, j.xt.data_ptr(), j.yt.data_ptr()), "add")
+        settle()
         check(bt.execute(s), "exec")
         s.synchronize()
         assert bt.take_status() == L.SIP_FFT_BATCH_GATE_TIMEOUT
         assert not j.result().any()
         flag.fill_(1)
+        settle()
         check(bt.execute(s), "exec")
         s.synchronize()
         assert bt.take_status() == 0
@@ -178,6 +183,7 @@ def test_graph_replay_with_changing_item_counts(cuda, jobs):
             for j in sel:
                 j.reset()
                 check(bt.add(j.h, j.xt.data_ptr(), j.yt.data_ptr()), "add")
+            settle()
             check(bt.execute(s), "exec")
             s.synchronize()
             assert bt.take_status() == 0

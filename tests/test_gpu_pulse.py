@@ -10,6 +10,7 @@ import pytest
 
 from oracle import oracle as O
 from sip_b200 import _lib as L
+from tests.fftcase import settle
 from tests.test_emu_pulse import signal
 
 pytestmark = pytest.mark.gpu
@@ -48,6 +49,7 @@ def test_pulse_vs_fp64_and_plain_chain(cuda, n, batch, flags):
     s = torch.cuda.Stream()
     p = Pulse(torch, n, batch, flags, 20261203 + n)
     check(p.h.set_stream(s), "stream")
+    settle()
     check(p.h.exec_c2c(p.xt, p.yt), "asdFftExecC2C")
     s.synchronize()
     out = p.yt.cpu().numpy()
@@ -61,9 +63,11 @@ def test_pulse_vs_fp64_and_plain_chain(cuda, n, batch, flags):
         check(h.set_stream(s), "stream")
     spec = torch.empty_like(p.xt)
     y2 = torch.empty_like(p.xt)
+    settle()
     check(fwd.exec_c2c(p.xt, spec), "fwd")
     with torch.cuda.stream(s):
         spec.mul_(p.ft.conj() if flags & 1 else p.ft)
+    settle()
     check(inv.exec_c2c(spec, y2), "inv")
     s.synchronize()
     plain = y2.cpu().numpy() / (n if flags & 2 else 1)
@@ -80,6 +84,7 @@ def test_pulse_in_place(cuda):
     for n in (4096, 65536):
         p = Pulse(torch, n, 3, 3, 7 + n)
         check(p.h.set_stream(s), "stream")
+        settle()
         check(p.h.exec_raw(p.xt.data_ptr(), p.xt.data_ptr()), "exec in place")
         s.synchronize()
         assert O.rel_l2(p.xt.cpu().numpy(), p.want()) <= REL_L2_TOL
@@ -99,6 +104,7 @@ def test_pulse_batched_queue_mix_equals_alone(cuda):
     with Batch(True) as bt:
         for p in ps:
             check(bt.add(p.h, p.xt.data_ptr(), p.yt.data_ptr()), "add")
+        settle()
         check(bt.execute(s), "exec")
         s.synchronize()
         assert bt.take_status() == 0
@@ -108,6 +114,7 @@ def test_pulse_batched_queue_mix_equals_alone(cuda):
         p.yt.zero_()
         with Batch(True) as bt:
             check(bt.add(p.h, p.xt.data_ptr(), p.yt.data_ptr()), "add")
+            settle()
             check(bt.execute(s), "exec")
             s.synchronize()
         np.testing.assert_array_equal(p.yt.cpu().numpy(), m)

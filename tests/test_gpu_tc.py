@@ -9,7 +9,7 @@ import pytest
 
 from oracle import oracle as O
 from sip_b200 import _lib as L
-from tests.fftcase import random_input
+from tests.fftcase import settle, random_input
 
 pytestmark = pytest.mark.gpu
 REL_L2_TOL = 1e-6
@@ -27,6 +27,7 @@ def _run(torch, n, batch, direction, x, mode):
         h.bind_workspace(dev)
         s = torch.cuda.Stream()
         check(h.set_stream(s), "stream")
+        settle()
         check(h.exec_c2c(xt, yt), "exec")
         check(h.synchronize(), "sync")
         desc = h.describe()

@@ -18,7 +18,7 @@ import pytest
 
 from oracle import oracle as O
 from sip_b200 import _lib as L
-from tests.fftcase import random_input
+from tests.fftcase import settle, random_input
 
 REL_L2_TOL = 1e-6
 
@@ -52,8 +52,10 @@ def test_no_alloc_matches_ordinary_exec(cuda, n, direction, batch):
         xt = torch.from_numpy(x).cuda()
         y_na = torch.zeros_like(xt)
         y_ref = torch.zeros_like(xt)
+        settle()
         check(lib.sipFftExecC2CNoAlloc(na.h, ctypes.c_void_p(xt.data_ptr()), ctypes.c_void_p(y_na.data_ptr())),
               "sipFftExecC2CNoAlloc")
+        settle()
         check(ref.exec_raw(xt.data_ptr(), y_ref.data_ptr()), "sipFftExecRaw")
         s.synchronize()
         a, b = y_na.cpu().numpy(), y_ref.cpu().numpy()
@@ -72,6 +74,7 @@ def test_no_alloc_rejects_oversized_and_non_c2c(cuda):
     big = plan(lib, n, O.FORWARD, batch, s)
     x = torch.zeros(batch * n, dtype=torch.complex64, device="cuda")
     y = torch.zeros_like(x)
+    settle()
     rc = lib.sipFftExecC2CNoAlloc(big.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()))
     assert rc == L.ACL_ERROR_INVALID_PARAM
     big.destroy()
@@ -79,6 +82,7 @@ def test_no_alloc_rejects_oversized_and_non_c2c(cuda):
 
     r2c = FftHandle()
     check(r2c.make_plan_1d(1000, O.R2C, O.FORWARD, 2), "plan")
+    settle()
     rc = lib.sipFftExecC2CNoAlloc(r2c.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()))
     assert rc == L.ACL_ERROR_API_NOT_SUPPORT
     r2c.destroy()
