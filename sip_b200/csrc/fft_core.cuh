@@ -330,7 +330,8 @@ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 // Read half of a pass: gather the butterflies this thread owns (butterfly
 // b = tid + s T over all P transforms of the tile), twiddle, transform.
 // `tw` is the plan's Stockham table of forward twiddles: for a pass with
-// span L > 1, entry pd.tw + k (R-1) + (r-1) is W_{L R}^{r k}.
+// span L > 1, entry pd.tw + (r-1) L + k is W_{L R}^{r k} (twiddle-major, so
+// the consecutive k of a warp read consecutive entries).
 template <int R, int SIGN, int S>
 SIP_HD void pass_read(int tid, int T, int P, int N, const float2* sm, int LD, const PassDesc& pd,
                       const float2* __restrict__ tw, PassRegs<R, S>& rg) {
@@ -347,9 +348,9 @@ SIP_HD void pass_read(int tid, int T, int P, int N, const float2* sm, int LD, co
             for (int r = 0; r < R; ++r) rg.v[s][r] = row[sidx(j + r * NR)];
             if (pd.L > 1) {
                 const int k = j - (int)fd_div(pd.l, (uint32_t)j) * pd.L;
-                const float2* w = tw + pd.tw + k * (R - 1);
+                const float2* w = tw + pd.tw + k;
 #pragma unroll
-                for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<SIGN>(rg.v[s][r], SIP_LDG(w + r - 1));
+                for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<SIGN>(rg.v[s][r], SIP_LDG(w + (r - 1) * pd.L));
             }
             dft<R, SIGN>(rg.v[s]);
         }

@@ -363,21 +363,21 @@ struct SkPass {
                 }
                 if constexpr (L > 1 && !K::TWB) {
                     const int k = j % L;
-                    const float2* w = a.tw + K::twoff(PASS) + k * (R - 1);
+                    const float2* w = a.tw + K::twoff(PASS) + k;  // twiddle-major table
 #pragma unroll
-                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + r - 1));
+                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + (r - 1) * L));
                 } else if constexpr (L > 1) {
                     // basis twiddles: W^{r k} = W^{r_lo k} W^{a r_hi k}
                     constexpr int A = basis_split(R);
                     const int k = j % L;
-                    const float2* w = a.tw + K::twoff(PASS) + k * basis_count(R);
+                    const float2* w = a.tw + K::twoff(PASS) + k;  // twiddle-major table
                     float2 lo[A], hi[R / A];
                     lo[0] = make_float2(1.f, 0.f);
                     hi[0] = make_float2(1.f, 0.f);
 #pragma unroll
-                    for (int t = 1; t < A; ++t) lo[t] = SIP_LDG(w + t - 1);
+                    for (int t = 1; t < A; ++t) lo[t] = SIP_LDG(w + (t - 1) * L);
 #pragma unroll
-                    for (int t = 1; t < R / A; ++t) hi[t] = SIP_LDG(w + A - 1 + t - 1);
+                    for (int t = 1; t < R / A; ++t) hi[t] = SIP_LDG(w + (A - 1 + t - 1) * L);
 #pragma unroll
                     for (int r = 1; r < R; ++r) {
                         const int rl = r % A, rh = r / A;

@@ -29,17 +29,19 @@ __global__ void k_stockham_tw(float2* out, const PlanDev plan, int entries) {
         if (pd.L <= 1) continue;
         const int cnt = pd.L * (pd.R - 1);
         if (i >= pd.tw && i < pd.tw + cnt) {
-            const int off = i - pd.tw;
-            const int k = off / (pd.R - 1);
-            const int r = off - k * (pd.R - 1) + 1;
+            const int off = i - pd.tw;  // twiddle-major: entry (r - 1) L + k
+            const int r = off / pd.L + 1;
+            const int k = off - (r - 1) * pd.L;
             out[i] = root_fwd((long long)r * k, (long long)pd.L * pd.R);
             return;
         }
     }
 }
 
-// Basis table (fft_core.cuh basis_split): per pass with span L > 1 and per
-// k < L, W_{LR}^{r k} for r = 1..a-1, then W_{LR}^{a h k} for h = 1..R/a-1.
+// Basis table (fft_core.cuh basis_split): per pass with span L > 1, the L
+// values of W_{LR}^{r k} (k < L) for r = 1..a-1, then of W_{LR}^{a h k} for
+// h = 1..R/a-1; twiddle-major, so the consecutive k of a warp's butterflies
+// read consecutive entries.
 __global__ void k_basis_tw(float2* out, const PlanDev plan, int entries) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= entries) return;
@@ -50,8 +52,8 @@ __global__ void k_basis_tw(float2* out, const PlanDev plan, int entries) {
         const int bc = basis_count(pd.R);
         const int cnt = pd.L * bc;
         if (i < off + cnt) {
-            const int k = (i - off) / bc;
-            const int t = (i - off) - k * bc;
+            const int t = (i - off) / pd.L;  // twiddle-major: entry t L + k
+            const int k = (i - off) - t * pd.L;
             const int a = basis_split(pd.R);
             const long long r = t < a - 1 ? t + 1 : (long long)a * (t - (a - 1) + 1);
             out[i] = root_fwd(r * k, (long long)pd.L * pd.R);

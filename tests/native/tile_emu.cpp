@@ -43,7 +43,7 @@ std::vector<float2> stockham_host(const PlanDev& pd) {
         const PassDesc& p = pd.pass[i];
         if (p.L <= 1) continue;
         for (int k = 0; k < p.L; ++k)
-            for (int r = 1; r < p.R; ++r) t[p.tw + k * (p.R - 1) + r - 1] = root_host((long long)r * k, (long long)p.L * p.R);
+            for (int r = 1; r < p.R; ++r) t[p.tw + (r - 1) * p.L + k] = root_host((long long)r * k, (long long)p.L * p.R);
     }
     return t;
 }
@@ -68,10 +68,10 @@ std::vector<float2> basis_host(const std::vector<int>& radices) {
     for (int R : radices) {
         if (L > 1) {
             const int a = basis_split(R);
-            for (int k = 0; k < L; ++k) {
-                for (int r = 1; r < a; ++r) t.push_back(root_host((long long)r * k, (long long)L * R));
-                for (int h = 1; h < R / a; ++h) t.push_back(root_host((long long)a * h * k, (long long)L * R));
-            }
+            for (int r = 1; r < a; ++r)
+                for (int k = 0; k < L; ++k) t.push_back(root_host((long long)r * k, (long long)L * R));
+            for (int h = 1; h < R / a; ++h)
+                for (int k = 0; k < L; ++k) t.push_back(root_host((long long)a * h * k, (long long)L * R));
         }
         L *= R;
     }
