@@ -87,19 +87,48 @@ __global__ void __launch_bounds__(kMaxTileThreads, 1)
     const int nitems = wave->items;
     const int total = wave->tiles;
     const QueueItem* items = items_base + wave->first;
+    // The descriptor of the item being worked on is kept in shared memory
+    // (the tile body reads its arguments many times), re-copied only when a
+    // claimed tile belongs to another item; the next tile is claimed while
+    // the current one is transformed.
+    __shared__ QueueItem s_item;
+    __shared__ int s_next, s_item_idx, s_copy;
+    if (threadIdx.x == 0) {
+        s_tile = (int)atomicAdd(counter, 1u);
+        s_item_idx = -1;
+    }
+    constexpr int kWords = (int)(sizeof(QueueItem) / sizeof(int));
+    static_assert(sizeof(QueueItem) % sizeof(int) == 0, "QueueItem copies as words");
     for (;;) {
-        if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
         __syncthreads();
         const int t = s_tile;
-        __syncthreads();
         if (t >= total) break;
-        int lo = 0, hi = nitems - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].tile_begin <= t) lo = mid;
-            else hi = mid - 1;
+        if (threadIdx.x == 0) {
+            int cur = s_item_idx;
+            const bool inside = cur >= 0 && t >= s_item.tile_begin && t < s_item.tile_begin + s_item.args.ntiles;
+            if (!inside) {
+                int lo = 0, hi = nitems - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (items[mid].tile_begin <= t) lo = mid;
+                    else hi = mid - 1;
+                }
+                cur = lo;
+            }
+            s_copy = inside ? -1 : cur;
+            s_item_idx = cur;
+            s_next = (int)atomicAdd(counter, 1u);
         }
-        q_dispatch(items + lo, t - items[lo].tile_begin);
+        __syncthreads();
+        const int copy = s_copy;
+        if (copy >= 0) {
+            const int* src = reinterpret_cast<const int*>(items + copy);
+            int* dst = reinterpret_cast<int*>(&s_item);
+            for (int w = threadIdx.x; w < kWords; w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+        }
+        q_dispatch(&s_item, t - s_item.tile_begin);  // ends with a barrier
+        if (threadIdx.x == 0) s_tile = s_next;
     }
 }
 
