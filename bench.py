@@ -403,9 +403,13 @@ def run_ours(args) -> None:
     single = [c for c in cands if c["kernels"] == 1]
     dom = max(single or cands, key=lambda c: c["ms"])
     traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
+    tfile = ROOT / "profiles" / "dram_traffic.md"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(dom["exec"].split(" rows")[0])
+        key = dom["exec"].split(" rows")[0]
+        for line in tfile.read_text().splitlines():
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 2 and cells[0] == key and cells[1].isdigit():
+                traffic = int(cells[1])
 
     # end to end through the C ABI from pinned host memory
     e2e = None
