@@ -47,6 +47,8 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_ELEMS_PER_THREAD 2 /* 16 or 32 */
 #define SIP_FFT_HINT_GENERIC_ONLY 3     /* 1: runtime-radix tile kernels only */
 #define SIP_FFT_HINT_RADIX_ORDER 4      /* 0: descending radices, 1: ascending */
+#define SIP_FFT_HINT_REAL_FUSED 5       /* real lengths above one tile: 0 default (R2C fused,
+                                           C2R pre-process pass), 1 fuse both, 2 fuse neither */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
 
 /* Pulse compression (matched filtering): plans y = IFFT(FFT(x) * F) for

@@ -42,6 +42,7 @@ SIP_FFT_HINT_TILE_TRANSFORMS = 1
 SIP_FFT_HINT_ELEMS_PER_THREAD = 2
 SIP_FFT_HINT_GENERIC_ONLY = 3
 SIP_FFT_HINT_RADIX_ORDER = 4
+SIP_FFT_HINT_REAL_FUSED = 5
 
 # Pulse-compression flags.
 SIP_FFT_PULSE_CONJ_FILTER = 1

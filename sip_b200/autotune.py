@@ -7,7 +7,7 @@ elements per thread and radix order (sipFftSetPlanHint).  Each candidate is
 planned, run `warmup` times and timed over `reps` executions with CUDA
 events on device-resident buffers; the fastest is appended to the tune
 cache, the file the planner reads at MakePlan when SIP_FFT_TUNE_CACHE names
-it.  Each line is "type direction dims batch P E generic order"
+it.  Each line is "type direction dims batch P E generic order fused"
 (dims like 64x128), and the last matching line wins.
 
 CLI: python -m sip_b200.autotune --type c2c --n 4096 --batch 256 --cache tune.txt
@@ -30,14 +30,16 @@ class Candidate:
     e: int = 0        # elements per thread (0: default)
     generic: int = 0  # 1: generic tile kernels only
     order: int = 0    # radix order (0 descending, 1 ascending)
+    fused: int = 0    # real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
 
     def line(self, fft_type: int, direction: int, sizes, batch: int) -> str:
         dims = "x".join(str(int(s)) for s in sizes)
-        return f"{fft_type} {direction} {dims} {batch} {self.p} {self.e} {self.generic} {self.order}\n"
+        return (f"{fft_type} {direction} {dims} {batch} {self.p} {self.e} {self.generic} {self.order} "
+                f"{self.fused}\n")
 
 
 def candidates(max_p: int = 16) -> list[Candidate]:
-    out = [Candidate()]
+    out = [Candidate(), Candidate(fused=1), Candidate(fused=2)]
     ps = [0] + [p for p in (1, 2, 4, 8, 16, 32) if p <= max_p]
     for p, e, order in itertools.product(ps, (16, 32), (0, 1)):
         out.append(Candidate(p, e, 1, order))
@@ -51,6 +53,7 @@ def apply(handle, c: Candidate) -> None:
     check(handle.set_hint(L.SIP_FFT_HINT_ELEMS_PER_THREAD, c.e), "hint E")
     check(handle.set_hint(L.SIP_FFT_HINT_GENERIC_ONLY, c.generic), "hint generic")
     check(handle.set_hint(L.SIP_FFT_HINT_RADIX_ORDER, c.order), "hint order")
+    check(handle.set_hint(L.SIP_FFT_HINT_REAL_FUSED, c.fused), "hint real fused")
 
 
 def _buffers(torch, fft_type: int, sizes, batch: int, device):
@@ -87,6 +90,7 @@ def time_candidate(torch, c: Candidate, fft_type: int, direction: int, sizes, ba
         h.bind_workspace(x.device)
         s = torch.cuda.Stream(device=x.device)
         check(h.set_stream(s), "stream")
+        torch.cuda.synchronize(x.device)  # inputs were filled on the default stream
         for _ in range(warmup):
             check(h.exec_raw(x.data_ptr(), y.data_ptr()), "exec")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

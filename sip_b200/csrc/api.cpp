@@ -602,6 +602,10 @@ AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
             if (value != 0 && value != 1) return ACL_ERROR_INVALID_PARAM;
             p->hint_order = value;
             break;
+        case SIP_FFT_HINT_REAL_FUSED:
+            if (value < 0 || value > 2) return ACL_ERROR_INVALID_PARAM;
+            p->hint_real_fused = value;
+            break;
         default:
             return ACL_ERROR_INVALID_PARAM;
     }

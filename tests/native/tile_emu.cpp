@@ -313,6 +313,10 @@ int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, lon
 
 int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_cap);
 
+// Planner real-fused hint applied to the plans emu_exec builds (0 default).
+static int g_emu_real_fused = 0;
+void emu_set_real_fused(int v) { g_emu_real_fused = v; }
+
 // Pulse-compression plan of length n over batch rows with the host filter
 // spectrum `filter` (n complex values) and flags (1 conj, 2 scale 1/n).
 int emu_exec_pulse(long long n, long long batch, const void* filter, int flags, const void* in, void* out,
@@ -342,6 +346,7 @@ int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, lon
     p.direction = static_cast<AsdSip::asdFftDirection>(direction);
     p.sizes.assign(sizes, sizes + ndim);
     p.batch = batch;
+    p.hint_real_fused = g_emu_real_fused;
     return emu_run_plan(p, in, out, desc, desc_cap);
 }
 

@@ -233,7 +233,7 @@ def test_partial_overlap_rejected(sip_lib, handle):
     (R2C, [1000], ["r2c half"]),
     (R2C, [2187], ["r2c pair"]),
     (R2C, [1 << 20], ["four-step A", "r2c four-step B + post"]),
-    (C2R, [1 << 20], ["c2r pre + four-step A", "four-step B"]),
+    (C2R, [1 << 20], ["c2r pre", "four-step A", "four-step B"]),
     (C2R, [64, 64], ["c2c axis 0", "c2r half"]),
 ])
 def test_plan_steps(sip_lib, handle, t, sizes, kinds):
@@ -307,3 +307,15 @@ def test_batch_api_without_device(sip_lib, handle):
     assert sip_lib.sipFftBatchAdd(None, handle, None, None) == INV
     assert sip_lib.sipFftBatchTakeStatus(None, None) == INV
     assert sip_lib.sipFftBatchSetGate(None, None, 0) == INV
+
+
+@pytest.mark.parametrize("t,value,kinds", [
+    (C2R, 1, ["c2r pre + four-step A", "four-step B"]),
+    (C2R, 2, ["c2r pre", "four-step A", "four-step B"]),
+    (R2C, 0, ["four-step A", "r2c four-step B + post"]),
+    (R2C, 2, ["four-step A", "four-step B", "r2c post"]),
+])
+def test_real_fused_hint(sip_lib, handle, t, value, kinds):
+    assert sip_lib.sipFftSetPlanHint(handle, L.SIP_FFT_HINT_REAL_FUSED, value) == OK
+    assert plan1d(sip_lib, handle, 1 << 20, t, F, 2) == OK
+    assert [s["what"].split(" n=")[0] for s in describe(sip_lib, handle)["steps"]] == kinds

@@ -4,6 +4,8 @@ tests/native/tile_emu.cpp, against the oracle.
 
 Covers every reference unit-test case plus plan kinds the GPU suite runs
 at full size only (four-step, large real, multi-D real, odd batches)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -126,10 +128,15 @@ def test_every_specialized_kernel(emu):
     matches the FP64 oracle (including partial tiles and odd row counts)."""
     entries = _sk_list(emu)
     assert len(entries) >= 20
+    emu.emu_set_real_fused.argtypes = [ctypes.c_int]
     for op, mode, sign, tw4, n, P, T in entries:
         typ, d, sizes, batch = _plan_for_sk(op, mode, sign, tw4, n)
         x = random_input(typ, sizes, batch, seed=n + op)
-        rc, out, desc = emu_run(emu, typ, d, sizes, batch, x)
+        emu.emu_set_real_fused(1 if op == 6 else 0)  # the fused C2R form is selected by hint
+        try:
+            rc, out, desc = emu_run(emu, typ, d, sizes, batch, x)
+        finally:
+            emu.emu_set_real_fused(0)
         assert rc == 0, desc
         import json
 

@@ -105,3 +105,33 @@ def test_specialized_kernels_many_tiles_per_cta(cuda, op, direction, n, batch):
     rows = np.unique(np.linspace(0, batch - 1, 24).astype(np.int64))
     err = O.rel_l2(out[rows], O.fp64(op, direction, x[rows], [n]))
     assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+
+
+# Both forms of the large real transforms (fused mirrored passes, or the
+# plain four-step plus a pre/post pass), selected with the planner hint.
+@pytest.mark.parametrize("op,direction", [(O.R2C, O.FORWARD), (O.C2R, O.INVERSE), (O.R2C, O.INVERSE),
+                                          (O.C2R, O.FORWARD)])
+@pytest.mark.parametrize("fused", [1, 2])
+def test_large_real_forms(cuda, op, direction, fused):
+    from sip_b200 import _lib as L
+    from sip_b200.fft import FftHandle, check
+    from tests.fftcase import settle
+
+    n, batch = 1 << 20, 3
+    ishape, idt, oshape, odt = shapes(op, [n], batch)
+    rng = np.random.default_rng(fused)
+    x = (rng.uniform(-1, 1, ishape).astype(np.float32) if idt == np.float32 else
+         (rng.standard_normal(ishape) + 1j * rng.standard_normal(ishape)).astype(np.complex64))
+    xt = cuda.from_numpy(x).cuda()
+    yt = cuda.zeros(oshape, dtype=cuda.complex64 if odt == np.complex64 else cuda.float32, device="cuda")
+    h = FftHandle()
+    check(h.set_hint(L.SIP_FFT_HINT_REAL_FUSED, fused), "hint")
+    check(h.make_plan_1d(n, op, direction, batch), "plan")
+    h.bind_workspace()
+    s = cuda.cuda.Stream()
+    check(h.set_stream(s), "stream")
+    settle()
+    check((h.exec_r2c if op == O.R2C else h.exec_c2r)(xt, yt), "exec")
+    s.synchronize()
+    assert O.rel_l2(yt.cpu().numpy(), O.fp64(op, direction, x, [n])) <= REL_L2_TOL
+    h.destroy()
