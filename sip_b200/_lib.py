@@ -43,6 +43,7 @@ SIP_FFT_HINT_ELEMS_PER_THREAD = 2
 SIP_FFT_HINT_GENERIC_ONLY = 3
 SIP_FFT_HINT_RADIX_ORDER = 4
 SIP_FFT_HINT_REAL_FUSED = 5
+SIP_FFT_HINT_SK_VARIANT = 6
 
 # Pulse-compression flags.
 SIP_FFT_PULSE_CONJ_FILTER = 1

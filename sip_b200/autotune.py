@@ -31,15 +31,16 @@ class Candidate:
     generic: int = 0  # 1: generic tile kernels only
     order: int = 0    # radix order (0 descending, 1 ascending)
     fused: int = 0    # real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
+    variant: int = 0  # compiled size-specialized variant
 
     def line(self, fft_type: int, direction: int, sizes, batch: int) -> str:
         dims = "x".join(str(int(s)) for s in sizes)
         return (f"{fft_type} {direction} {dims} {batch} {self.p} {self.e} {self.generic} {self.order} "
-                f"{self.fused}\n")
+                f"{self.fused} {self.variant}\n")
 
 
 def candidates(max_p: int = 16) -> list[Candidate]:
-    out = [Candidate(), Candidate(fused=1), Candidate(fused=2)]
+    out = [Candidate(), Candidate(fused=1), Candidate(fused=2)] + [Candidate(variant=v) for v in (1, 2, 3)]
     ps = [0] + [p for p in (1, 2, 4, 8, 16, 32) if p <= max_p]
     for p, e, order in itertools.product(ps, (16, 32), (0, 1)):
         out.append(Candidate(p, e, 1, order))
@@ -54,6 +55,7 @@ def apply(handle, c: Candidate) -> None:
     check(handle.set_hint(L.SIP_FFT_HINT_GENERIC_ONLY, c.generic), "hint generic")
     check(handle.set_hint(L.SIP_FFT_HINT_RADIX_ORDER, c.order), "hint order")
     check(handle.set_hint(L.SIP_FFT_HINT_REAL_FUSED, c.fused), "hint real fused")
+    check(handle.set_hint(L.SIP_FFT_HINT_SK_VARIANT, c.variant), "hint sk variant")
 
 
 def _buffers(torch, fft_type: int, sizes, batch: int, device):

@@ -606,6 +606,10 @@ AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
             if (value < 0 || value > 2) return ACL_ERROR_INVALID_PARAM;
             p->hint_real_fused = value;
             break;
+        case SIP_FFT_HINT_SK_VARIANT:
+            if (value < 0 || value > 15) return ACL_ERROR_INVALID_PARAM;
+            p->hint_sk_variant = value;
+            break;
         default:
             return ACL_ERROR_INVALID_PARAM;
     }

@@ -44,7 +44,7 @@ int64_t FftPlan::elements() const {
 // API lock).
 namespace {
 int g_compute_mode = kComputeFp32;
-int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0;
+int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0, g_hint_variant = 0;
 }  // namespace
 
 // ------------------------------------------------------------ radices
@@ -200,7 +200,7 @@ void try_specialize(Step& st, const AxisIO& io) {
     TileArgs& a = L.args;
     const int mode = sk_mode_of(L.op, a.N, io);
     if (mode < 0) return;
-    const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N);
+    const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
     if (e == nullptr) return;
     st.sk = e;
     st.radices = e->radices;
@@ -577,8 +577,10 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr || g_hint_generic;
     const bool fuse = g_hint_real_fused == 1 || (g_hint_real_fused == 0 && r2c);
     if (split && !generic_only && fuse) {
-        const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1) : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1);
-        const SkEntry* eb = r2c ? sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2) : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
+        const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1)
+                                : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1, g_hint_variant);
+        const SkEntry* eb = r2c ? sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2, g_hint_variant)
+                                : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
         if (ea != nullptr && eb != nullptr) {
             if (r2c) {
                 C2COpts o;
@@ -687,18 +689,19 @@ bool apply_tune_cache(FftPlan& plan) {
     char line[512];
     bool hit = false;
     while (std::fgets(line, sizeof(line), f)) {
-        int type = 0, dir = 0, p = 0, e = 0, gen = 0, order = 0, fused = 0;
+        int type = 0, dir = 0, p = 0, e = 0, gen = 0, order = 0, fused = 0, variant = 0;
         long long batch = 0;
         char d[256] = {0};
-        const int got =
-            std::sscanf(line, "%d %d %255s %lld %d %d %d %d %d", &type, &dir, d, &batch, &p, &e, &gen, &order, &fused);
-        if (got != 8 && got != 9) continue;
+        const int got = std::sscanf(line, "%d %d %255s %lld %d %d %d %d %d %d", &type, &dir, d, &batch, &p, &e, &gen,
+                                    &order, &fused, &variant);
+        if (got < 8) continue;
         if (type == (int)plan.type && dir == (int)plan.direction && dims == d && batch == plan.batch) {
             plan.hint_p = p;
             plan.hint_e = e;
             plan.hint_generic = gen;
             plan.hint_order = order;
-            plan.hint_real_fused = got == 9 ? fused : 0;
+            plan.hint_real_fused = got >= 9 ? fused : 0;
+            plan.hint_sk_variant = got >= 10 ? variant : 0;
             hit = true;  // the last matching line wins
         }
     }
@@ -713,6 +716,7 @@ void build_steps(FftPlan& plan) {
     g_hint_generic = plan.hint_generic;
     g_hint_order = plan.hint_order;
     g_hint_real_fused = plan.hint_real_fused;
+    g_hint_variant = plan.hint_sk_variant;
     plan.steps.clear();
     plan.workspace_need = 0;
     if (plan.pulse) {

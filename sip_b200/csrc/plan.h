@@ -77,6 +77,7 @@ struct FftPlan {
     int hint_generic = 0;  // 1: generic tile kernels only (no size-specialized / tensor-core)
     int hint_order = 0;    // radix order: 0 descending, 1 ascending
     int hint_real_fused = 0;  // real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
+    int hint_sk_variant = 0;  // which compiled size-specialized variant (sk_configs.h order)
     bool hints_explicit = false;
     // Pulse-compression plan (sipFftMakePlanPulse1D): x -> IFFT(FFT(x) * F)
     // per row, F a device spectrum of length sizes[0] owned by the caller.
@@ -115,7 +116,8 @@ void build_steps(FftPlan& plan);
 void prepare_device(FftPlan& plan);
 
 // Applies the tune-cache entry for the plan (file named by SIP_FFT_TUNE_CACHE,
-// lines "type direction n0[xn1[xn2]] batch P E generic order [real_fused]");
+// lines "type direction n0[xn1[xn2]] batch P E generic order [real_fused
+// [sk_variant]]");
 // returns true
 // when an entry matched.
 bool apply_tune_cache(FftPlan& plan);

@@ -4,7 +4,10 @@
 // that the kernel does not spill.  TWB selects basis (1) or full (0) pass
 // twiddles (sk_kernel.cuh SkCfg::TWB).
 // Every other length runs on the generic tile kernel.  The shard index
-// spreads the instantiations over parallel compile units.
+// spreads the instantiations over parallel compile units.  Several entries
+// for the same (N, OP, MODE, SIGN, TW4) are variants of the tile shape or
+// register target: the first is the planner's default, the others are
+// selected by the sk-variant planner hint (and timed by the autotuner).
 #pragma once
 
 #define SIP_SK_CONFIGS(X)                                                     \
@@ -34,16 +37,23 @@
     X(3, 512, 16, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 1, 16, 32)                    \
     X(4, 1024, 8, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 32, 32)                \
     X(5, 1024, 8, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 32, 32)                 \
-    /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000) */      \
+    /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000); the   \
+       first entry of each is the default, the second a hint variant */     \
+    X(0, 500, 4, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 1, 25, 20)              \
     X(6, 500, 8, 200, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 20)              \
+    X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 1, 25, 20)               \
     X(7, 500, 8, 200, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 20)               \
+    X(2, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 1, 25, 15, 8)          \
     X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 15, 8)          \
     X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 15, 8)           \
+    X(3, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 1, 25, 15, 8)           \
     /* odd real length 2187 = 3^7, two rows per complex FFT */                \
     X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 1, 27, 9, 9)           \
-    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)        \
-    /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A */      \
-    X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)      \
+    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
+    /* real 2^20 fused four-step: R2C pass B + post (and a smaller-tile      \
+       variant), C2R pre + pass A (planner hint) */                          \
+    X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)            \
+    X(6, 1024, 8, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 3, 1, 32, 32)             \
     X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)
 
 #define SIP_SK_SHARDS 8

@@ -1,4 +1,6 @@
 // Lookup of the size-specialized kernels compiled by the sk_shard units.
+#include <algorithm>
+
 #include "sk_configs.h"
 #include "sk_registry.h"
 
@@ -24,15 +26,20 @@ const std::vector<SkEntry>& sk_registry() {
         sk_register_shard_5(v);
         sk_register_shard_6(v);
         sk_register_shard_7(v);
+        std::stable_sort(v.begin(), v.end(), [](const SkEntry& a, const SkEntry& b) { return a.order < b.order; });
         return v;
     }();
     return reg;
 }
 
-const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n) {
-    for (const SkEntry& e : sk_registry())
-        if (e.op == op && e.mode == mode && e.sign == sign && e.tw4 == tw4 && e.n == n) return &e;
-    return nullptr;
+const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant) {
+    const SkEntry* first = nullptr;
+    for (const SkEntry& e : sk_registry()) {
+        if (e.op != op || e.mode != mode || e.sign != sign || e.tw4 != tw4 || e.n != n) continue;
+        if (first == nullptr) first = &e;
+        if (variant-- == 0) return &e;
+    }
+    return first;
 }
 
 }  // namespace sipfft

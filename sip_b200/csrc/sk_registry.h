@@ -20,10 +20,13 @@ struct SkEntry {
     int LD;
     int smem;        // dynamic shared memory per CTA (bytes)
     const void* fn;  // kernel (library) or CPU runner (test harness)
+    int order = 0;   // position in the SIP_SK_CONFIGS list
 };
 
-// Entry for (op, mode, sign, tw4, n), or nullptr.
-const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n);
+// The `variant`-th entry compiled for (op, mode, sign, tw4, n) in
+// SIP_SK_CONFIGS order (0: the default); the default when that variant is
+// not compiled; nullptr when no entry is.
+const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant = 0);
 
 const std::vector<SkEntry>& sk_registry();
 

@@ -32,12 +32,17 @@ SkEntry make_entry(std::vector<int> radices) {
     return e;
 }
 
+// Registers this shard's entries, each with its position in the
+// SIP_SK_CONFIGS list (the registry is ordered by it).
 template <int SHARD>
 void register_shard(std::vector<SkEntry>& out) {
+    int order = 0;
 #define SIP_SK_ENTRY(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, ...)                                  \
     if constexpr (S == SHARD) {                                                                                   \
         out.push_back(make_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, TWB, __VA_ARGS__>, STAGES>({__VA_ARGS__})); \
-    }
+        out.back().order = order;                                                                                 \
+    }                                                                                                             \
+    ++order;
     SIP_SK_CONFIGS(SIP_SK_ENTRY)
 #undef SIP_SK_ENTRY
 }

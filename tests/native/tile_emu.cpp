@@ -167,11 +167,15 @@ const std::vector<SkEntry>& sk_registry() {
     }();
     return reg;
 }
-const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n) {
+const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant) {
     if (std::getenv("SIP_EMU_GENERIC_ONLY")) return nullptr;
-    for (const SkEntry& e : sk_registry())
-        if (e.op == op && e.mode == mode && e.sign == sign && e.tw4 == tw4 && e.n == n) return &e;
-    return nullptr;
+    const SkEntry* first = nullptr;
+    for (const SkEntry& e : sk_registry()) {
+        if (e.op != op || e.mode != mode || e.sign != sign || e.tw4 != tw4 || e.n != n) continue;
+        if (first == nullptr) first = &e;
+        if (variant-- == 0) return &e;
+    }
+    return first;
 }
 }  // namespace sipfft
 
@@ -316,6 +320,9 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
 // Planner real-fused hint applied to the plans emu_exec builds (0 default).
 static int g_emu_real_fused = 0;
 void emu_set_real_fused(int v) { g_emu_real_fused = v; }
+// Planner sk-variant hint applied likewise.
+static int g_emu_sk_variant = 0;
+void emu_set_sk_variant(int v) { g_emu_sk_variant = v; }
 
 // Pulse-compression plan of length n over batch rows with the host filter
 // spectrum `filter` (n complex values) and flags (1 conj, 2 scale 1/n).
@@ -347,6 +354,7 @@ int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, lon
     p.sizes.assign(sizes, sizes + ndim);
     p.batch = batch;
     p.hint_real_fused = g_emu_real_fused;
+    p.hint_sk_variant = g_emu_sk_variant;
     return emu_run_plan(p, in, out, desc, desc_cap);
 }
 

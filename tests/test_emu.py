@@ -129,20 +129,27 @@ def test_every_specialized_kernel(emu):
     entries = _sk_list(emu)
     assert len(entries) >= 20
     emu.emu_set_real_fused.argtypes = [ctypes.c_int]
+    emu.emu_set_sk_variant.argtypes = [ctypes.c_int]
+    seen = {}
     for op, mode, sign, tw4, n, P, T in entries:
         typ, d, sizes, batch = _plan_for_sk(op, mode, sign, tw4, n)
         x = random_input(typ, sizes, batch, seed=n + op)
+        key = (op, mode, sign, tw4, n)
+        variant = seen.get(key, 0)  # later entries of the same kernel are hint-selected variants
+        seen[key] = variant + 1
         emu.emu_set_real_fused(1 if op == 6 else 0)  # the fused C2R form is selected by hint
+        emu.emu_set_sk_variant(variant)
         try:
             rc, out, desc = emu_run(emu, typ, d, sizes, batch, x)
         finally:
             emu.emu_set_real_fused(0)
+            emu.emu_set_sk_variant(0)
         assert rc == 0, desc
         import json
 
         steps = json.loads(desc)["steps"]
         hit = [s for s in steps if s.get("sk") and s["n"] == n and s["op"] == op and s["sign"] == sign
-               and s["tw4"] == bool(tw4)]
+               and s["tw4"] == bool(tw4) and s["P"] * (2 if op in (5, 6) else 1) == P and s["threads"] == T]
         assert hit, (op, mode, sign, tw4, n, desc[:400])
         err = O.rel_l2(out, O.fp64(typ, d, x, sizes))
         assert err <= REL_L2_TOL, (op, mode, sign, tw4, n, err)
