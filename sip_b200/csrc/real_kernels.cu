@@ -8,31 +8,42 @@ namespace sipfft {
 
 namespace {
 
-// One thread per pair (k, m - k), k in [0, m/2]: each value is read once.
+// One thread per pair (k, m - k), k in [0, m/2]: each value and each
+// twiddle is read once (the mirror's twiddle follows from W_{2m}^k).
 __global__ void k_real_post(const RealPassArgs a) {
     const long long pairs = a.m / 2 + 1;
+    const bool cj = a.conj != 0;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
         const float2* z = a.src + row * a.in_pitch;
         float2* x = a.dst + row * a.out_pitch;
         for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pairs;
              k += (long long)gridDim.x * blockDim.x) {
-            x[k] = real_post_elem(z, k, a.m, a.tw, a.conj != 0);
             const long long km = a.m - k;
-            if (km != k) x[km] = real_post_elem(z, km, a.m, a.tw, a.conj != 0);
+            if (k > 0 && k < km) {
+                real_post_pair(z, k, a.m, a.tw, cj, x + k, x + km);
+            } else {
+                x[k] = real_post_elem(z, k, a.m, a.tw, cj);
+                if (km != k) x[km] = real_post_elem(z, km, a.m, a.tw, cj);
+            }
         }
     }
 }
 
 __global__ void k_real_pre(const RealPassArgs a) {
     const long long pairs = a.m / 2 + 1;
+    const bool cj = a.conj != 0;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
         const float2* x = a.src + row * a.in_pitch;
         float2* z = a.dst + row * a.out_pitch;
         for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pairs;
              k += (long long)gridDim.x * blockDim.x) {
-            z[k] = real_pre_elem(x, k, a.m, a.tw, a.conj != 0);
             const long long km = a.m - k;
-            if (km != k && km < a.m) z[km] = real_pre_elem(x, km, a.m, a.tw, a.conj != 0);
+            if (k > 0 && k < km) {
+                real_pre_pair(x, k, a.m, a.tw, cj, z + k, z + km);
+            } else {
+                z[k] = real_pre_elem(x, k, a.m, a.tw, cj);
+                if (km != k && km < a.m) z[km] = real_pre_elem(x, km, a.m, a.tw, cj);
+            }
         }
     }
 }

@@ -39,4 +39,44 @@ SIP_HD float2 real_pre_elem(const float2* x, long long k, long long m, const flo
     return make_float2(e.x - od.y, e.y + od.x);
 }
 
+// X[k] and X[m - k] for 0 < k < m - k: one read of z[k], z[m - k] and
+// W_{2m}^k; the mirror uses W_{2m}^{m-k} = -conj(W_{2m}^k), so
+// X[m - k] = conj(ev - W od) where X[k] = ev + W od.
+SIP_HD void real_post_pair(const float2* z, long long k, long long m, const float2* tw, bool conj, float2* xk,
+                           float2* xmk) {
+    const float2 zk = SIP_LDG(z + k);
+    const float2 zm = SIP_LDG(z + m - k);
+    const float2 b = make_float2(zm.x, -zm.y);
+    const float2 ev = make_float2(0.5f * (zk.x + b.x), 0.5f * (zk.y + b.y));
+    const float2 od = make_float2(0.5f * (zk.y - b.y), -0.5f * (zk.x - b.x));
+    const float2 t = c_mul(SIP_LDG(tw + k), od);
+    float2 v = c_add(ev, t);
+    float2 w = make_float2(ev.x - t.x, -(ev.y - t.y));
+    if (conj) {
+        v.y = -v.y;
+        w.y = -w.y;
+    }
+    *xk = v;
+    *xmk = w;
+}
+
+// Z[k] and Z[m - k] for 0 < k < m - k from x[k], x[m - k] and W_{2m}^k:
+// with Z[k] = e + i W^{-k} d (e, d from x[k] and conj x[m - k]), the mirror
+// is Z[m - k] = conj(e) + conj(i W^{-k} d) (its e is conj(e), its d is
+// -conj(d), and W^{-(m-k)} = -conj(W^{-k})).
+SIP_HD void real_pre_pair(const float2* x, long long k, long long m, const float2* tw, bool conj, float2* zk,
+                          float2* zmk) {
+    float2 xv = SIP_LDG(x + k), yv = SIP_LDG(x + m - k);
+    if (conj) {
+        xv.y = -xv.y;
+        yv.y = -yv.y;
+    }
+    const float2 b = make_float2(yv.x, -yv.y);
+    const float2 e = make_float2(0.5f * (xv.x + b.x), 0.5f * (xv.y + b.y));
+    const float2 d = make_float2(0.5f * (xv.x - b.x), 0.5f * (xv.y - b.y));
+    const float2 od = c_mulc(d, SIP_LDG(tw + k));
+    *zk = make_float2(e.x - od.y, e.y + od.x);
+    *zmk = make_float2(e.x + od.y, -e.y + od.x);
+}
+
 }  // namespace sipfft

@@ -50,10 +50,9 @@
     /* odd real length 2187 = 3^7, two rows per complex FFT */                \
     X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 1, 27, 9, 9)           \
     X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
-    /* real 2^20 fused four-step: R2C pass B + post (and a smaller-tile      \
-       variant), C2R pre + pass A (planner hint) */                          \
+    /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A        \
+       (planner hint) */                                                     \
     X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)            \
-    X(6, 1024, 8, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 3, 1, 32, 32)             \
     X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)
 
 #define SIP_SK_SHARDS 8

@@ -293,13 +293,28 @@ void emu_real_step(const Step& st, const void* src, void* dst) {
     const RealPassArgs& r = st.real;
     const float2* s = static_cast<const float2*>(src);
     float2* d = static_cast<float2*>(dst);
+    // the kernels' pairing (real_kernels.cu): pair functions for 0 < k < m - k
+    const bool cj = r.conj != 0;
     for (long long row = 0; row < r.rows; ++row) {
-        if (st.kind == StepKind::RealPost) {
-            for (long long k = 0; k <= r.m; ++k)
-                d[row * r.out_pitch + k] = real_post_elem(s + row * r.in_pitch, k, r.m, tw.data(), r.conj != 0);
-        } else {
-            for (long long k = 0; k < r.m; ++k)
-                d[row * r.out_pitch + k] = real_pre_elem(s + row * r.in_pitch, k, r.m, tw.data(), r.conj != 0);
+        const float2* in = s + row * r.in_pitch;
+        float2* out = d + row * r.out_pitch;
+        for (long long k = 0; k <= r.m / 2; ++k) {
+            const long long km = r.m - k;
+            if (st.kind == StepKind::RealPost) {
+                if (k > 0 && k < km) {
+                    real_post_pair(in, k, r.m, tw.data(), cj, out + k, out + km);
+                } else {
+                    out[k] = real_post_elem(in, k, r.m, tw.data(), cj);
+                    if (km != k) out[km] = real_post_elem(in, km, r.m, tw.data(), cj);
+                }
+            } else {
+                if (k > 0 && k < km) {
+                    real_pre_pair(in, k, r.m, tw.data(), cj, out + k, out + km);
+                } else {
+                    out[k] = real_pre_elem(in, k, r.m, tw.data(), cj);
+                    if (km != k && km < r.m) out[km] = real_pre_elem(in, km, r.m, tw.data(), cj);
+                }
+            }
         }
     }
 }
