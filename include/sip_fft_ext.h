@@ -49,6 +49,8 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_RADIX_ORDER 4      /* 0: descending radices, 1: ascending */
 #define SIP_FFT_HINT_REAL_FUSED 5       /* real lengths above one tile: 0 default (R2C fused,
                                            C2R pre-process pass), 1 fuse both, 2 fuse neither */
+#define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant
+                                           (0 default; a step without that variant uses its default) */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
 
 /* Pulse compression (matched filtering): plans y = IFFT(FFT(x) * F) for
