@@ -238,6 +238,66 @@ def precision_form(torch, dev, stream, steps: int, warmup: int) -> dict:
     return out
 
 
+def other_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> dict:
+    """The reference's other benchmark configurations, forward and inverse,
+    device-resident, CUDA events: 1D C2C N=4096 x 256 (16.8 MB, so 12
+    rotating buffer pairs keep every timed exec's data out of L2), 2D C2C
+    2048 x 2048 x 8 and 3D C2C 256^3 (one HBM pass per axis).  Inputs
+    i.i.d. N(0, 1), seed 20261029 + N; rel-L2 against the FP64 oracle on the
+    first transform.  `gbs_moved` counts one read and one write of the data
+    per pass (the bandwidth the passes reach), `gbs_algorithmic` one of each
+    per transform."""
+    from oracle import oracle as O
+    from sip_b200 import _lib as L
+    from sip_b200.fft import FftHandle, check
+
+    out = {}
+    for name, sizes, batch, nbuf in (("c2c_4096_b256", [4096], 256, 12), ("c2c_2d_2048x2048_b8", [2048, 2048], 8, 1),
+                                     ("c2c_3d_256^3", [256, 256, 256], 1, 1)):
+        g = torch.Generator(device=dev)
+        g.manual_seed(SEED + sizes[0])
+        shape = (batch,) + tuple(sizes)
+        xs = [torch.complex(torch.randn(shape, generator=g, device=dev), torch.randn(shape, generator=g, device=dev))
+              for _ in range(nbuf)]
+        ys = [torch.empty_like(x) for x in xs]
+        elems = batch * math.prod(sizes)
+        flops = 5 * elems * math.log2(math.prod(sizes))
+        res = {}
+        for d, dname in ((L.ASCEND_FFT_FORWARD, "fwd"), (L.ASCEND_FFT_INVERSE, "inv")):
+            h = FftHandle()
+            if len(sizes) == 1:
+                check(h.make_plan_1d(sizes[0], L.ASCEND_FFT_C2C, d, batch), "plan")
+            elif len(sizes) == 2:
+                check(h.make_plan_2d(sizes[0], sizes[1], L.ASCEND_FFT_C2C, d, batch), "plan")
+            else:
+                check(h.make_plan_3d(*sizes, L.ASCEND_FFT_C2C, d, batch), "plan")
+            h.bind_workspace(dev)
+            check(h.set_stream(stream), "stream")
+            passes = len(h.describe()["steps"])
+            torch.cuda.synchronize()
+            for i in range(warmup):
+                check(h.exec_raw(xs[i % nbuf].data_ptr(), ys[i % nbuf].data_ptr()), "exec")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(steps):
+                check(h.exec_raw(xs[i % nbuf].data_ptr(), ys[i % nbuf].data_ptr()), "exec")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            check(h.exec_raw(xs[0].data_ptr(), ys[0].data_ptr()), "exec")
+            torch.cuda.synchronize()
+            x0 = xs[0][:1].cpu().numpy()
+            err = O.rel_l2(ys[0][:1].cpu().numpy(), O.fp64(O.C2C, d, x0, sizes))
+            res[dname] = {"ms": round(ms, 4), "passes": passes,
+                          "gbs_moved": round(16 * elems * passes / (ms * 1e-3) / 1e9, 1),
+                          "gbs_algorithmic": round(16 * elems / (ms * 1e-3) / 1e9, 1),
+                          "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "rel_l2": float(f"{err:.3e}")}
+            h.destroy()
+        out[name] = res
+        del xs, ys
+    return out
+
+
 def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
     """Serving form: Poisson pulse-compression requests (N log-uniform over
     2,3,5-smooth lengths in [256, 2^18], batch uniform 1..512, delayed chirp
@@ -458,6 +518,9 @@ def run_ours(args) -> None:
     prec = None
     if rank == 0 and not args.no_precision:
         prec = precision_form(torch, dev, stream, steps=5, warmup=2)
+    others = None
+    if rank == 0 and not args.no_other:
+        others = other_configs(torch, dev, stream)
     serve = None
     if rank == 0 and not args.no_serve:
         serve = serving(torch, args.serve_requests)
@@ -484,6 +547,7 @@ def run_ours(args) -> None:
             "cpu_baseline": cpu,
             "precision_form": prec,
             "serving": serve,
+            "other_configs": others,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
         }
@@ -508,6 +572,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 vs tensor-core comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-form comparison")
+    ap.add_argument("--no-other", action="store_true", help="skip the 1D/2D/3D C2C configurations")
     ap.add_argument("--serve-requests", type=int, default=3000, help="requests per serving run")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")
     ap.add_argument("--ref-seconds", type=float, default=1.5, help="reference arm seconds per size per step")
