@@ -53,6 +53,18 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
                                            (0 default; a step without that variant uses its default) */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
 
+/* fftshift / ifftshift fused into the transform's output store (after
+ * Create, before MakePlan; C2C 1-D and 2-D plans): mode 1 rotates every
+ * output slice as asdFftShift does ((n+1)/2 per axis), mode 2 as
+ * asdIfftShift (n/2 per axis), each value times `scale`; mode 0 turns it
+ * off.  1-D slices are 1 x N; 2-D slices are X x Y, and the plan then needs
+ * a workspace of batch * X * Y * 8 bytes.  Saves the separate shift pass the
+ * reference runs (core/fft/fftshift.cpp). */
+#define SIP_FFT_SHIFT_NONE 0
+#define SIP_FFT_SHIFT_FFTSHIFT 1
+#define SIP_FFT_SHIFT_IFFTSHIFT 2
+AsdSip::AspbStatus sipFftSetOutputShift(AsdSip::asdFftHandle handle, int mode, double scale);
+
 /* Pulse compression (matched filtering): plans y = IFFT(FFT(x) * F) for
  * `batch` complex64 rows of length n, with F the filter spectrum (n complex64
  * values in device memory, owned by the caller and read at exec time).

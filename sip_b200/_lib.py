@@ -45,6 +45,11 @@ SIP_FFT_HINT_RADIX_ORDER = 4
 SIP_FFT_HINT_REAL_FUSED = 5
 SIP_FFT_HINT_SK_VARIANT = 6
 
+# Output shift modes (sipFftSetOutputShift).
+SIP_FFT_SHIFT_NONE = 0
+SIP_FFT_SHIFT_FFTSHIFT = 1
+SIP_FFT_SHIFT_IFFTSHIFT = 2
+
 # Pulse-compression flags.
 SIP_FFT_PULSE_CONJ_FILTER = 1
 SIP_FFT_PULSE_SCALE = 2
@@ -66,7 +71,7 @@ EXPORTED = [
     "sipFftExecRaw", "sipFftDescribePlan", "sipFftVersion", "sipFftSetComputeMode", "sipFftTakeDeviceErrors",
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
-    "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows",
+    "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows", "sipFftSetOutputShift",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -113,6 +118,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftExecC2CNoAlloc": (_i32, [_vp, _vp, _vp]),
         "sipFftMakePlanPulse1D": (_i32, [_vp, _i64, _i64, _vp, ctypes.c_int]),
         "sipFftBatchAddRows": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
+        "sipFftSetOutputShift": (_i32, [_vp, ctypes.c_int, ctypes.c_double]),
         "aclCreateTensor": (_vp, [ctypes.POINTER(_i64), ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_i64), _i64,
                                   ctypes.c_int, ctypes.POINTER(_i64), ctypes.c_uint64, _vp]),
         "aclDestroyTensor": (ctypes.c_int, [_vp]),

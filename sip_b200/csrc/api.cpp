@@ -722,6 +722,15 @@ AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status) {
     return ACL_SUCCESS;
 }
 
+AspbStatus sipFftSetOutputShift(asdFftHandle handle, int mode, double scale) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || p->initialized || mode < 0 || mode > 2) return ACL_ERROR_INVALID_PARAM;
+    p->out_shift = mode;
+    p->out_scale = scale;
+    return ACL_SUCCESS;
+}
+
 AspbStatus sipFftMakePlanPulse1D(asdFftHandle handle, int64_t fftSize, int64_t batchSize, const void* filter,
                                  int flags) {
     std::lock_guard<std::mutex> lk(g_mu);

@@ -478,6 +478,71 @@ void add_pulse(FftPlan& plan) {
     plan.workspace_need = (size_t)(batch * n * 8);
 }
 
+// Sets the fftshift epilogue on the step that writes the output: each
+// output slice of rows x cols is rotated as asdFftShift (mode 1) or
+// asdIfftShift (mode 2) would, and scaled.
+void set_out_shift(Step& st, const FftPlan& plan, long long rows, long long cols) {
+    TileArgs& a = st.L.args;
+    a.flags |= TF_SHIFT_OUT;
+    a.sh_rows = (int)rows;
+    a.sh_cols = (int)cols;
+    a.sh_slice = rows * cols;
+    a.sh_r = (int)(plan.out_shift == 1 ? (rows + 1) / 2 : rows / 2);
+    a.sh_c = (int)(plan.out_shift == 1 ? (cols + 1) / 2 : cols / 2);
+    a.div_sh_cols = make_fastdiv((uint32_t)cols);
+    if (plan.out_scale != 1.0) {
+        a.flags |= TF_SCALE;
+        a.scale = (float)plan.out_scale;
+    }
+    st.what += " + shift";
+}
+
+// C2C with the fftshift epilogue (1-D: slices of 1 x N; 2-D: slices of
+// X x Y).  The rotation moves values across tiles, so the step that writes
+// the output reads from another buffer: 1-D rows and the four-step pass B
+// already do; 2-D runs its row pass into the workspace and the column pass
+// from there into the output.  Generic tile kernels only.
+void add_shifted_c2c(FftPlan& plan) {
+    if (plan.type != ASCEND_FFT_C2C || plan.sizes.size() > 2)
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "output shift is for 1-D and 2-D C2C plans");
+    g_hint_generic = 1;
+    const long long b = plan.batch;
+    if (plan.sizes.size() == 1) {
+        const long long n = plan.sizes[0];
+        add_c2c_1d(plan, n, b, C2COpts{});
+        set_out_shift(plan.steps.back(), plan, 1, n);
+        return;
+    }
+    const long long X = plan.sizes[0], Y = plan.sizes[1];
+    if (X > kMaxTileN || Y > kMaxTileN || X * Y > 0x7fffffffLL)
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
+    AxisIO r;
+    r.inner = b * X;
+    r.in_idist = Y;
+    r.out_idist = Y;
+    Step rows = make_tile_step(OP_C2C, c2c_sign(plan), (int)Y, (int)Y, false, r, 0, 0,
+                               "c2c axis 1 n=" + std::to_string(Y));
+    rows.src = Loc::In;
+    rows.dst = Loc::Ws;
+    plan.steps.push_back(rows);
+    AxisIO c;
+    c.inner = Y;
+    c.outer = b;
+    c.in_odist = X * Y;
+    c.in_idist = 1;
+    c.in_stride = Y;
+    c.out_odist = X * Y;
+    c.out_idist = 1;
+    c.out_stride = Y;
+    Step cols = make_tile_step(OP_C2C, c2c_sign(plan), (int)X, (int)X, true, c, 0, 0,
+                               "c2c axis 0 n=" + std::to_string(X));
+    cols.src = Loc::Ws;
+    cols.dst = Loc::Out;
+    set_out_shift(cols, plan, X, Y);
+    plan.steps.push_back(cols);
+    plan.workspace_need = (size_t)(b * X * Y * 8);
+}
+
 // Real transform along contiguous rows of length n (rows rows), one tile.
 void add_real_rows(FftPlan& plan, bool r2c, long long n, long long rows, Loc src, Loc dst) {
     const long long h = n / 2 + 1;
@@ -721,6 +786,10 @@ void build_steps(FftPlan& plan) {
     plan.workspace_need = 0;
     if (plan.pulse) {
         add_pulse(plan);
+        return;
+    }
+    if (plan.out_shift != 0) {
+        add_shifted_c2c(plan);
         return;
     }
     if (plan.type == ASCEND_FFT_C2C_SEP) {

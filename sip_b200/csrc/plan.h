@@ -81,6 +81,10 @@ struct FftPlan {
     bool hints_explicit = false;
     // Pulse-compression plan (sipFftMakePlanPulse1D): x -> IFFT(FFT(x) * F)
     // per row, F a device spectrum of length sizes[0] owned by the caller.
+    // Output rotation (sipFftSetOutputShift): 0 none, 1 fftshift, 2 ifftshift
+    // of every (1 x N) or (X x Y) output slice, times out_scale.
+    int out_shift = 0;
+    double out_scale = 1.0;
     bool pulse = false;
     const void* pulse_filter = nullptr;
     int pulse_flags = 0;  // SIP_FFT_PULSE_CONJ_FILTER | SIP_FFT_PULSE_SCALE

@@ -55,6 +55,7 @@ enum TileFlags : int {
     TF_MUL_CONJ = 16, // use conj(mul[...]) (TF_MUL and OP_PC)
     TF_PLANAR_IN = 32,   // C2C input as two float planes: src (real), src_im (imaginary)
     TF_PLANAR_OUT = 64,  // C2C output as two float planes: dst (real), dst_im (imaginary)
+    TF_SHIFT_OUT = 128,  // C2C output rotated per slice of sh_rows x sh_cols (fftshift epilogue)
 };
 
 struct TileArgs {
@@ -78,6 +79,10 @@ struct TileArgs {
     const float2* mul;       // TF_MUL spectrum (e.g. a matched filter)
     const float* src_im;     // TF_PLANAR_IN imaginary plane
     float* dst_im;           // TF_PLANAR_OUT imaginary plane
+    long long sh_slice;      // TF_SHIFT_OUT: elements per slice (sh_rows x sh_cols)
+    int sh_rows, sh_cols;    //   slice shape
+    int sh_r, sh_c;          //   row / column rotation
+    FastDiv div_sh_cols;     //   / sh_cols
     long long mul_pitch_p, mul_pitch_k;
     float scale;
     FastDiv div_n;           // / N
@@ -179,6 +184,21 @@ SIP_HD float2 cross_tw(const TileArgs& a, long long m) {
     return c_mul(lo, hi);
 }
 
+// TF_SHIFT_OUT: position of output element f (flat index into the output
+// array of slices) after rotating its slice by (sh_r, sh_c), the layout of
+// asdFftShift / asdIfftShift applied to the transform's output.
+SIP_HD long long shifted_index(const TileArgs& a, long long f) {
+    const long long s = f / a.sh_slice;
+    const int rem = (int)(f - s * a.sh_slice);
+    const int row = (int)fd_div(a.div_sh_cols, (uint32_t)rem);
+    const int col = rem - row * a.sh_cols;
+    int r2 = row + a.sh_r;
+    if (r2 >= a.sh_rows) r2 -= a.sh_rows;
+    int c2 = col + a.sh_c;
+    if (c2 >= a.sh_cols) c2 -= a.sh_cols;
+    return s * a.sh_slice + (long long)r2 * a.sh_cols + c2;
+}
+
 // ------------------------------------------------------------ C2C store
 // TW4: multiply element k of transform p by W_N^{(i0 + p) k} (the four-step
 // cross twiddle).
@@ -199,6 +219,16 @@ SIP_HD void store_c2c(int tid, int T, const TileArgs& a, const TileCtx& c, const
     float2* dst = static_cast<float2*>(a.dst);
     const int N = a.N, P = a.P;
 #define SIP_C2C_VALUE(p_, n_) c2c_out_value<SIGN, TW4>(a, c, sm, (p_), (n_))
+    if (a.flags & TF_SHIFT_OUT) {
+        const int total = c.cnt * N;
+        for (int f = tid; f < total; f += T) {
+            const int p = (int)fd_div(a.div_n, (uint32_t)f);
+            const int n = f - p * N;
+            const long long i = c.out_base + (long long)p * a.out_idist + (long long)n * a.out_stride;
+            dst[shifted_index(a, i)] = SIP_C2C_VALUE(p, n);
+        }
+        return;
+    }
     if (a.flags & TF_PLANAR_OUT) {
         float* re = static_cast<float*>(a.dst);
         const int total = c.cnt * N;

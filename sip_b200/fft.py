@@ -83,6 +83,10 @@ class FftHandle:
     def make_plan_1d(self, n, fft_type, direction, batch, dim_type=L.ASCEND_FFT_HORIZONTAL) -> int:
         return self.lib.asdFftMakePlan1D(self.h, n, fft_type, direction, batch, dim_type)
 
+    def set_output_shift(self, mode: int, scale: float = 1.0) -> int:
+        """sipFftSetOutputShift: fftshift (1) / ifftshift (2) fused into the output store."""
+        return self.lib.sipFftSetOutputShift(self.h, mode, scale)
+
     def make_plan_pulse_1d(self, n, batch, filter_ptr: int, flags: int = 0) -> int:
         """sipFftMakePlanPulse1D: y = IFFT(FFT(x) * F) per row; F lives on the
         device at filter_ptr (n complex64 values) and must outlive the plan."""

@@ -338,6 +338,13 @@ void emu_set_real_fused(int v) { g_emu_real_fused = v; }
 // Planner sk-variant hint applied likewise.
 static int g_emu_sk_variant = 0;
 void emu_set_sk_variant(int v) { g_emu_sk_variant = v; }
+// Output shift (mode, scale) applied likewise.
+static int g_emu_shift = 0;
+static double g_emu_shift_scale = 1.0;
+void emu_set_out_shift(int mode, double scale) {
+    g_emu_shift = mode;
+    g_emu_shift_scale = scale;
+}
 
 // Pulse-compression plan of length n over batch rows with the host filter
 // spectrum `filter` (n complex values) and flags (1 conj, 2 scale 1/n).
@@ -370,6 +377,8 @@ int emu_exec_mode(int type, int direction, int ndim, const long long* sizes, lon
     p.batch = batch;
     p.hint_real_fused = g_emu_real_fused;
     p.hint_sk_variant = g_emu_sk_variant;
+    p.out_shift = g_emu_shift;
+    p.out_scale = g_emu_shift_scale;
     return emu_run_plan(p, in, out, desc, desc_cap);
 }
 
