@@ -39,6 +39,8 @@ UNITS = [
     ("batch.cpp", [], "batch.o"),
     ("noalloc.cu", [], "noalloc.o"),
     ("shift.cu", [], "shift.o"),
+    ("bluestein.cu", [], "bluestein.o"),
+    ("bluestein_host.cpp", [], "bluestein_host.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),

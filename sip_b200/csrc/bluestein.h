@@ -1,0 +1,25 @@
+// Bluestein pre/post passes and tables (bluestein.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "bluestein.cuh"
+
+namespace sipfft {
+
+cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream);
+cudaError_t bluestein_post(const BluesteinArgs& a, cudaStream_t stream);
+
+// Chirp c_j = exp(sign i pi (j^2 mod 2n) / n), j < n (FP64, rounded once).
+cudaError_t gen_chirp(float2* out, long long n, int sign, cudaStream_t stream);
+
+// Convolution filter FFT_m(b), b_j = conj(c_j), b_{m-j} = b_j (j < n),
+// computed on the host in FP64 and rounded once.
+std::vector<float2> bluestein_filter(long long n, long long m, int sign);
+
+// Smallest 2,3,5-smooth m >= 2n - 1.
+long long bluestein_length(long long n);
+
+}  // namespace sipfft

@@ -26,7 +26,8 @@ void check(cudaError_t e, const char* what) {
 
 struct TableKey {
     int device;
-    int kind;  // 0 stockham, 1 roots, 2 basis, 3 split cross twiddles, 4 tensor-core B operand
+    int kind;  // 0 stockham, 1 roots, 2 basis, 3 split cross twiddles, 4 tensor-core B operand,
+               // 5 Bluestein chirp, 6 Bluestein filter
     long long a, b;
     std::vector<int> radices;
     bool operator<(const TableKey& o) const {
@@ -125,12 +126,46 @@ BufPtr split_table(int device, long long n, int shift) {
     return b;
 }
 
+BufPtr chirp_table(int device, long long n, int sign) {
+    TableKey key{device, 5, n, sign, {}};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    BufPtr b = alloc_buf((size_t)n * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_chirp(static_cast<float2*>(b->ptr), n, sign, s); });
+    g_tables[key] = b;
+    return b;
+}
+
+BufPtr blue_filter_table(int device, long long n, long long m, int sign) {
+    TableKey key{device, 6, n, m * 2 + (sign > 0 ? 1 : 0), {}};
+    std::lock_guard<std::mutex> lk(g_table_mu);
+    auto it = g_tables.find(key);
+    if (it != g_tables.end())
+        if (auto sp = it->second.lock()) return sp;
+    const std::vector<float2> host = bluestein_filter(n, m, sign);
+    BufPtr b = alloc_buf(host.size() * sizeof(float2), device);
+    check(cudaMemcpy(b->ptr, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice), "cudaMemcpy");
+    g_tables[key] = b;
+    return b;
+}
+
 }  // namespace
 
 void prepare_device(FftPlan& plan) {
     int device = -1;
     check(cudaGetDevice(&device), "cudaGetDevice");
     for (Step& st : plan.steps) {
+        if (st.kind == StepKind::Blue) {
+            st.chirp_buf = chirp_table(device, st.blue_n, st.blue_sign);
+            st.blue.chirp = static_cast<const float2*>(st.chirp_buf->ptr);
+            continue;
+        }
+        if (st.mul_table == 1) {
+            st.mul_buf = blue_filter_table(device, st.blue_n, st.blue_m, st.blue_sign);
+            st.L.args.mul = static_cast<const float2*>(st.mul_buf->ptr);
+        }
         if (st.tw2_kind == 1) st.tw2 = root_table(device, st.tw2_n, st.tw2_count);
         if (st.tw2_kind == 2) st.tw2 = split_table(device, st.tw2_n, st.L.args.tw4_shift);
         if (st.kind == StepKind::RealPost || st.kind == StepKind::RealPre) {
@@ -197,6 +232,11 @@ void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
         char* dst = resolve(st.dst, st.dst_off);
         if (st.kind == StepKind::Tile) {
             check(tile_launch(st.L, src, dst, stream), "tile kernel launch");
+        } else if (st.kind == StepKind::Blue) {
+            BluesteinArgs a = st.blue;
+            a.src = src;
+            a.dst = dst;
+            check(st.blue_post ? bluestein_post(a, stream) : bluestein_pre(a, stream), "bluestein pass launch");
         } else if (st.kind == StepKind::Tc) {
             check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
                             st.L.args.tw, stream),

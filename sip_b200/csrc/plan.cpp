@@ -402,11 +402,18 @@ void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
 //   pass C: n1-point inverse FFTs down the columns into y[m2 + n2 m1].
 // Three HBM round trips instead of five (forward four-step, multiply,
 // inverse four-step), and no transposed store.
-void add_pulse(FftPlan& plan) {
-    const long long n = plan.sizes[0], batch = plan.batch;
-    const bool cj = (plan.pulse_flags & kPulseConj) != 0;
-    const bool sc = (plan.pulse_flags & kPulseScale) != 0;
-    const auto* filt = static_cast<const float2*>(plan.pulse_filter);
+// Operand placement of a pulse chain: input, output, and the four-step
+// intermediate (workspace offset), so the chain also runs on workspace
+// buffers (Bluestein's convolution).
+struct PulseIO {
+    Loc src = Loc::In, dst = Loc::Out;
+    size_t src_off = 0, dst_off = 0, scratch_off = 0;
+    int mul_table = 0;  // 1: the filter is the plan's Bluestein table (set at device preparation)
+};
+
+void add_pulse_steps(FftPlan& plan, long long n, long long batch, const float2* filt, int flags, const PulseIO& pio) {
+    const bool cj = (flags & kPulseConj) != 0;
+    const bool sc = (flags & kPulseScale) != 0;
     const int mul_flags = cj ? TF_MUL_CONJ : 0;
     const int out_flags = sc ? TF_SCALE : 0;
     const float scale = 1.0f / (float)n;
@@ -422,6 +429,11 @@ void add_pulse(FftPlan& plan) {
         st.L.args.mul_pitch_k = 1;
         st.L.args.scale = scale;
         st.batch_dim = 1;
+        st.src = pio.src;
+        st.dst = pio.dst;
+        st.src_off = pio.src_off;
+        st.dst_off = pio.dst_off;
+        st.mul_table = pio.mul_table;
         plan.steps.push_back(st);
         return;
     }
@@ -446,8 +458,10 @@ void add_pulse(FftPlan& plan) {
     sa.tw2_kind = 2;
     sa.tw2_n = n;
     sa.tw2_count = split_count;
-    sa.src = Loc::In;
+    sa.src = pio.src;
+    sa.src_off = pio.src_off;
     sa.dst = Loc::Ws;
+    sa.dst_off = pio.scratch_off;
     AxisIO r;  // rows of Y, in place
     r.inner = n1;
     r.outer = batch;
@@ -466,16 +480,25 @@ void add_pulse(FftPlan& plan) {
     sp.L.args.mul_pitch_k = n1;
     sp.src = Loc::Ws;
     sp.dst = Loc::Ws;
+    sp.src_off = sp.dst_off = pio.scratch_off;
+    sp.mul_table = pio.mul_table;
     Step sc3 = make_tile_step(OP_C2C, 1, n1, n1, true, a, out_flags, 0,
                               "pulse inverse columns n=" + std::to_string(n) + " n1=" + std::to_string(n1));
     sc3.L.args.scale = scale;
     sc3.src = Loc::Ws;
-    sc3.dst = Loc::Out;
+    sc3.src_off = pio.scratch_off;
+    sc3.dst = pio.dst;
+    sc3.dst_off = pio.dst_off;
     sa.batch_dim = sp.batch_dim = sc3.batch_dim = 2;
     plan.steps.push_back(sa);
     plan.steps.push_back(sp);
     plan.steps.push_back(sc3);
-    plan.workspace_need = (size_t)(batch * n * 8);
+    plan.workspace_need = std::max(plan.workspace_need, pio.scratch_off + (size_t)(batch * n * 8));
+}
+
+void add_pulse(FftPlan& plan) {
+    add_pulse_steps(plan, plan.sizes[0], plan.batch, static_cast<const float2*>(plan.pulse_filter),
+                    plan.pulse_flags, PulseIO{});
 }
 
 // Sets the fftshift epilogue on the step that writes the output: each
@@ -541,6 +564,67 @@ void add_shifted_c2c(FftPlan& plan) {
     set_out_shift(cols, plan, X, Y);
     plan.steps.push_back(cols);
     plan.workspace_need = (size_t)(b * X * Y * 8);
+}
+
+// Lengths the radix passes handle directly (the rest take Bluestein).
+bool c2c_direct(long long n) {
+    if (n <= kMaxTileN) return factorizable((int)n, 32);
+    int n1 = 0, n2 = 0;
+    return four_step_split(n, &n1, &n2);
+}
+
+bool real_direct(long long n) {
+    if (n % 2 == 0) return c2c_direct(n / 2);
+    return n <= kMaxTileN && factorizable((int)n, 32);
+}
+
+constexpr long long kMaxBluesteinN = 1LL << 22;
+
+// Bluestein's algorithm (bluestein.cuh): pre pass into the workspace, the
+// fused pulse chain of length m in place there (filter = the plan's
+// Bluestein table, scale 1/m), post pass into the output.  Workspace:
+// [0, conv) the convolution rows, then the four-step intermediate of m.
+void add_bluestein(FftPlan& plan, int kind, long long n, long long batch) {
+    if (n > kMaxBluesteinN)
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " needs Bluestein above 2^22");
+    const long long m = bluestein_length(n);
+    const int sign = plan.forward() ? -1 : 1;
+    const size_t conv = ((size_t)(batch * m * 8) + 255) / 256 * 256;
+    Step pre;
+    pre.kind = StepKind::Blue;
+    pre.blue.n = n;
+    pre.blue.m = m;
+    pre.blue.rows = batch;
+    pre.blue.kind = kind;
+    pre.blue.in_pitch = kind == BLUE_C2R ? n / 2 + 1 : n;
+    pre.blue.out_pitch = m;
+    pre.blue_n = n;
+    pre.blue_m = m;
+    pre.blue_sign = sign;
+    pre.src = Loc::In;
+    pre.dst = Loc::Ws;
+    pre.what = "bluestein pre n=" + std::to_string(n) + " m=" + std::to_string(m);
+    plan.steps.push_back(pre);
+    const size_t first = plan.steps.size();
+    PulseIO pio;
+    pio.src = pio.dst = Loc::Ws;
+    pio.scratch_off = conv;
+    pio.mul_table = 1;
+    add_pulse_steps(plan, m, batch, nullptr, kPulseScale, pio);
+    for (size_t i = first; i < plan.steps.size(); ++i) {
+        plan.steps[i].blue_n = n;
+        plan.steps[i].blue_m = m;
+        plan.steps[i].blue_sign = sign;
+    }
+    Step post = pre;
+    post.blue_post = true;
+    post.blue.in_pitch = m;
+    post.blue.out_pitch = kind == BLUE_R2C ? n / 2 + 1 : n;
+    post.src = Loc::Ws;
+    post.dst = Loc::Out;
+    post.what = "bluestein post n=" + std::to_string(n);
+    plan.steps.push_back(post);
+    plan.workspace_need = std::max(plan.workspace_need, conv + (m > kMaxTileN ? (size_t)(batch * m * 8) : 0));
 }
 
 // Real transform along contiguous rows of length n (rows rows), one tile.
@@ -808,6 +892,14 @@ void build_steps(FftPlan& plan) {
     const bool r2c = plan.type == ASCEND_FFT_R2C;
     if (sz.size() == 1) {
         const long long n = sz[0];
+        if (plan.type == ASCEND_FFT_C2C && !c2c_direct(n)) {
+            add_bluestein(plan, BLUE_C2C, n, b);
+            return;
+        }
+        if (!c2c && !real_direct(n)) {
+            add_bluestein(plan, r2c ? BLUE_R2C : BLUE_C2R, n, b);
+            return;
+        }
         if (c2c) {
             add_c2c_1d(plan, n, b, C2COpts{});
         } else if (real_fits_tile(n)) {
@@ -896,6 +988,9 @@ std::string describe(const FftPlan& plan) {
                << ",\"radices\":[";
             for (size_t r = 0; r < st.radices.size(); ++r) os << (r ? "," : "") << st.radices[r];
             os << "]";
+        } else if (st.kind == StepKind::Blue) {
+            os << ",\"n\":" << st.blue.n << ",\"m\":" << st.blue.m << ",\"rows\":" << st.blue.rows
+               << ",\"post\":" << (st.blue_post ? "true" : "false");
         } else {
             os << ",\"m\":" << st.real.m << ",\"rows\":" << st.real.rows << ",\"conj\":" << st.real.conj;
         }

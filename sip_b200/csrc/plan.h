@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "fft_api.h"
+#include "bluestein.h"
 #include "real_kernels.h"
 #include "sk_registry.h"
 #include "tile_launch.h"
@@ -41,7 +42,7 @@ using BufPtr = std::shared_ptr<DeviceBuf>;
 // Operand of a step.
 enum class Loc : int { In = 0, Out = 1, Ws = 2 };
 
-enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2, Tc = 3 };
+enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2, Tc = 3, Blue = 4 };
 
 struct Step {
     StepKind kind = StepKind::Tile;
@@ -52,6 +53,15 @@ struct Step {
     // Which tile index the plan's batch runs along (for executing fewer rows
     // than planned through the batch queue): 0 neither, 1 inner, 2 outer.
     int batch_dim = 0;
+    // Bluestein: pre / post pass arguments (kind Blue), and on the pulse
+    // steps of the convolution mul_table = 1 (filter FFT_m(b) of length blue_m
+    // for transform length blue_n and sign blue_sign, made at device preparation).
+    BluesteinArgs blue{};
+    bool blue_post = false;
+    int mul_table = 0;
+    long long blue_n = 0, blue_m = 0;
+    int blue_sign = 0;
+    BufPtr mul_buf, chirp_buf;
     PlanDev host_plan{};              // pass list (uploaded to plan_dev)
     std::vector<int> radices;
     int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count

@@ -17,7 +17,7 @@ NVCC = "/usr/local/cuda/bin/nvcc"
 
 
 def build() -> Path:
-    srcs = [HERE / "tile_emu.cpp", CSRC / "plan.cpp"]
+    srcs = [HERE / "tile_emu.cpp", CSRC / "plan.cpp", CSRC / "bluestein_host.cpp"]
     deps = srcs + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").rglob("*.h"))
     if LIB.exists() and LIB.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
         return LIB

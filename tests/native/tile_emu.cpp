@@ -288,6 +288,31 @@ void emu_tc_step(const Step& st, const void* src, void* dst) {
 #undef SIP_EMU_TC
 }
 
+// Bluestein pre / post pass on the CPU (bluestein.cuh element functions)
+// with the chirp computed on the host.
+void emu_blue_step(const Step& st, const void* src, void* dst) {
+    const long long n = st.blue_n;
+    std::vector<float2> chirp(n);
+    for (long long j = 0; j < n; ++j) {
+        const long long q = (j * j) % (2 * n);
+        const long double a = 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
+        chirp[j] = make_float2((float)std::cos(a), (float)(st.blue_sign * std::sin(a)));
+    }
+    BluesteinArgs a = st.blue;
+    a.src = src;
+    a.dst = dst;
+    a.chirp = chirp.data();
+    if (!st.blue_post) {
+        float2* out = static_cast<float2*>(dst);
+        for (long long row = 0; row < a.rows; ++row)
+            for (long long j = 0; j < a.m; ++j) out[row * a.m + j] = blue_pre_elem(a, row, j);
+    } else {
+        const long long cnt = blue_out_count(a);
+        for (long long row = 0; row < a.rows; ++row)
+            for (long long k = 0; k < cnt; ++k) blue_post_elem(a, row, k);
+    }
+}
+
 void emu_real_step(const Step& st, const void* src, void* dst) {
     std::vector<float2> tw = tw2_host(st);
     const RealPassArgs& r = st.real;
@@ -401,7 +426,17 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
             };
             char* s = resolve(st.src, st.src_off);
             char* d = resolve(st.dst, st.dst_off);
-            if (st.kind == StepKind::Tile) emu_tile_step(st, s, d);
+            std::vector<float2> filt;
+            Step stc;
+            const Step* use = &st;
+            if (st.mul_table == 1) {  // the Bluestein filter the device preparation would make
+                filt = bluestein_filter(st.blue_n, st.blue_m, st.blue_sign);
+                stc = st;
+                stc.L.args.mul = filt.data();
+                use = &stc;
+            }
+            if (st.kind == StepKind::Blue) emu_blue_step(st, s, d);
+            else if (use->kind == StepKind::Tile) emu_tile_step(*use, s, d);
             else if (st.kind == StepKind::Tc) emu_tc_step(st, s, d);
             else emu_real_step(st, s, d);
         }

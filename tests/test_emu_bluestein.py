@@ -1,0 +1,35 @@
+"""Lengths with a prime factor above 32 run Bluestein's algorithm
+(bluestein.cuh): CPU harness against the FP64 oracle, C2C / R2C / C2R,
+both directions, single-tile and four-step convolution lengths."""
+import json
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.fftcase import emu_run, random_input
+
+REL_L2_TOL = 1e-6
+LENGTHS = [37, 67, 97, 629, 1009, 2018, 4099, 20011]
+
+
+@pytest.mark.parametrize("n", LENGTHS)
+@pytest.mark.parametrize("op", [O.C2C, O.R2C, O.C2R])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_bluestein_harness(emu, n, op, direction):
+    batch = 3
+    x = random_input(op, [n], batch, seed=n + op)
+    if op == O.C2R:  # a genuine half spectrum (imaginary DC / Nyquist ignored as numpy does)
+        x = np.fft.rfft(np.random.default_rng(n).uniform(-1, 1, (batch, n))).astype(np.complex64)
+    rc, out, desc = emu_run(emu, op, direction, [n], batch, x)
+    assert rc == 0, desc
+    kinds = [s["what"].split(" n=")[0] for s in json.loads(desc)["steps"]]
+    assert kinds[0] == "bluestein pre" and kinds[-1] == "bluestein post", kinds
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, err
+
+
+def test_direct_lengths_do_not_use_bluestein(emu):
+    x = random_input(O.C2C, [1000], 2)
+    rc, _, desc = emu_run(emu, O.C2C, O.FORWARD, [1000], 2, x)
+    assert rc == 0 and "bluestein" not in desc
