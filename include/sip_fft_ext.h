@@ -90,8 +90,9 @@ AsdSip::AspbStatus sipFftMakePlanPulse1D(AsdSip::asdFftHandle handle, int64_t n,
  * set and the launch does no work); TakeStatus reads and clears the status
  * word.  Only plans whose passes are all tile passes are accepted (C2C of any
  * length, real transforms up to one tile per row); others give
- * ACL_ERROR_API_NOT_SUPPORT.  None of these has a counterpart in the
- * reference. */
+ * ACL_ERROR_API_NOT_SUPPORT.  The batch keeps pointers into the added plans'
+ * device tables: a plan must stay alive until every exec it was added to has
+ * completed.  None of these has a counterpart in the reference. */
 typedef void* sipFftBatch;
 AsdSip::AspbStatus sipFftBatchCreate(sipFftBatch* batch);
 AsdSip::AspbStatus sipFftBatchDestroy(sipFftBatch batch);

@@ -40,11 +40,13 @@ int64_t FftPlan::elements() const {
     return e;
 }
 
-// Compute mode and hints of the plan being built (build_steps runs under the
-// API lock).
+// Compute mode and hints of the plan being built, set by build_steps for the
+// helpers below (per thread, so concurrent planners do not interfere; the C
+// ABI also plans under its global lock).
 namespace {
-int g_compute_mode = kComputeFp32;
-int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0, g_hint_variant = 0;
+thread_local int g_compute_mode = kComputeFp32;
+thread_local int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0,
+                 g_hint_variant = 0;
 }  // namespace
 
 // ------------------------------------------------------------ radices
