@@ -305,14 +305,15 @@ def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
     admission budget.  The plain per-request FP32 path (forward C2C,
     multiply, inverse C2C, LRU(10) plan cache) is first run with every
     request present at t=0 to measure its capacity; then both paths serve
-    the same arrival sequence at 0.8x and 2x that capacity.  A bounded
+    the same arrival sequence at 0.8x and 2x that capacity; the queue's own
+    capacity is measured the same way.  A bounded
     sample of `count` requests stands in for the 100k-request stream."""
     from oracle import oracle as O
     from sip_b200.serve import KIND_PULSE, PlainExecutor, QueueExecutor, Scheduler, make_requests, smooth_lengths
 
     budget = int(budget_gb * (1 << 30))
     lengths = smooth_lengths(256, 1 << 18)
-    queue = QueueExecutor(torch, budget, lengths, max_batch=512, streams=3)
+    queue = QueueExecutor(torch, budget, lengths, max_batch=512, streams=4)
     plain = PlainExecutor(torch, budget, cache_size=10)
     errs = []
 
@@ -333,6 +334,8 @@ def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
     cap = Scheduler(plain, budget, max_inflight=64, max_group=1).run(
         make_requests(count, rate_hz=float("inf"))).summary()
     out["plain_capacity"] = cap
+    out["queue_capacity"] = Scheduler(queue, budget, max_inflight=3).run(
+        make_requests(count, rate_hz=float("inf"))).summary()
     rate_cap = cap["throughput_req_s"]
     for f in (0.8, 2.0):
         rate = f * rate_cap

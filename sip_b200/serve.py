@@ -340,6 +340,7 @@ class QueueExecutor(_GpuBase):
         self.max_batch = max_batch
         self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
         self.batches = [Batch(use_graphs) for _ in range(streams)]
+        self.slot_event = [None] * streams
         self.next = 0
         self.plans = {}
         for n in lengths:
@@ -354,9 +355,20 @@ class QueueExecutor(_GpuBase):
                 self.plans[(kind, n)] = h
         self.launches = 0
 
+    def _free_slot(self) -> int:
+        """A stream / batch slot whose last group has completed (a batch
+        object's next exec waits for its previous one on the host), else the
+        least recently used one."""
+        for k in range(len(self.streams)):
+            i = (self.next + k) % len(self.streams)
+            ev = self.slot_event[i]
+            if ev is None or ev.query():
+                return i
+        return self.next
+
     def launch(self, group):
         torch = self.torch
-        i = self.next
+        i = self._free_slot()
         self.next = (i + 1) % len(self.streams)
         s = self.streams[i]
         bt = self.batches[i]
@@ -372,6 +384,7 @@ class QueueExecutor(_GpuBase):
         check(bt.execute(s), "batch exec")
         ev = torch.cuda.Event(enable_timing=True)
         ev.record(s)
+        self.slot_event[i] = ev
         self.launches += 1
         return ev
 
