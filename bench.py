@@ -353,6 +353,89 @@ def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
     return out
 
 
+def run_e2e(torch, dev, plans, stream, ke: int, step_flops: float, world: int, dist) -> dict:
+    """The round trip from pinned host memory through the C ABI, as an
+    application streams it: every size is cut into chunks of rows; chunk i's
+    host-to-device copy (one stream), its R2C + C2R (the compute stream) and
+    chunk i-1's device-to-host copy (a third stream) overlap, with two
+    device buffers per stage.  Every input byte crosses PCIe once each way
+    inside the timed region."""
+    from sip_b200 import _lib as L
+    from sip_b200.fft import FftHandle, check
+    from sip_b200.replicas import max_over_ranks
+
+    chunks_per_size = 8
+    s_in, s_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    host_in = [p["x"].cpu().pin_memory() for p in plans]
+    host_out = [torch.empty(p["y"].shape, dtype=torch.float32).pin_memory() for p in plans]
+    work = []   # (size index, first row, rows, r2c handle, c2r handle)
+    handles = {}
+    for i, p in enumerate(plans):
+        n, rows = p["n"], p["rows"]
+        step = -(-rows // chunks_per_size)
+        for r0 in range(0, rows, step):
+            rc = min(step, rows - r0)
+            if (n, rc) not in handles:
+                hr, hc = FftHandle(), FftHandle()
+                check(hr.make_plan_1d(n, L.ASCEND_FFT_R2C, L.ASCEND_FFT_FORWARD, rc), "plan r2c")
+                check(hc.make_plan_1d(n, L.ASCEND_FFT_C2R, L.ASCEND_FFT_INVERSE, rc), "plan c2r")
+                for h in (hr, hc):
+                    h.bind_workspace(dev)
+                    check(h.set_stream(stream), "stream")
+                handles[(n, rc)] = (hr, hc)
+            work.append((i, r0, rc) + handles[(n, rc)])
+    big_in = max(rc * plans[i]["n"] for i, _, rc, _, _ in work)
+    big_spec = max(rc * (plans[i]["n"] // 2 + 1) for i, _, rc, _, _ in work)
+    din = [torch.empty(big_in, dtype=torch.float32, device=dev) for _ in range(2)]
+    dspec = [torch.empty(big_spec, dtype=torch.complex64, device=dev) for _ in range(2)]
+    dout = [torch.empty(big_in, dtype=torch.float32, device=dev) for _ in range(2)]
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_comp = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+
+    def one_step():
+        for g, (i, r0, rc, hr, hc) in enumerate(work):
+            k = g % 2
+            n = plans[i]["n"]
+            cnt = rc * n
+            s_in.wait_event(ev_comp[k])          # din[k] free: compute of chunk g-2 done
+            with torch.cuda.stream(s_in):
+                din[k][:cnt].copy_(host_in[i][r0:r0 + rc].reshape(-1), non_blocking=True)
+            ev_in[k].record(s_in)
+            stream.wait_event(ev_in[k])
+            stream.wait_event(ev_out[k])         # dout[k] free: copy-out of chunk g-2 done
+            check(hr.exec_raw(din[k].data_ptr(), dspec[k].data_ptr()), "exec r2c")
+            check(hc.exec_raw(dspec[k].data_ptr(), dout[k].data_ptr()), "exec c2r")
+            ev_comp[k].record(stream)
+            s_out.wait_event(ev_comp[k])
+            with torch.cuda.stream(s_out):
+                host_out[i][r0:r0 + rc].reshape(-1).copy_(dout[k][:cnt], non_blocking=True)
+            ev_out[k].record(s_out)
+
+    one_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s_in)
+    for _ in range(ke):
+        one_step()
+    s_out.wait_event(ev_comp[0])
+    s_out.wait_event(ev_comp[1])
+    e1.record(s_out)
+    torch.cuda.synchronize()
+    e_ms = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
+    for p, hi, ho in zip(plans, host_in, host_out):  # the round trip returns the input (times N)
+        assert np.allclose(ho[:2].numpy() / p["n"], hi[:2].numpy(), atol=1e-5)
+        assert np.allclose(ho[-2:].numpy() / p["n"], hi[-2:].numpy(), atol=1e-5)
+    for hr, hc in handles.values():
+        hr.destroy()
+        hc.destroy()
+    hb = sum(t.numel() * 4 for t in host_in)
+    db = sum(t.numel() * 4 for t in host_out)
+    return {"value": round(world * step_flops / (e_ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+            "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "steps": ke,
+            "pipeline": f"{chunks_per_size} chunks per size, copy-in / compute / copy-out on three streams"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args) -> None:
     import torch
@@ -477,36 +560,7 @@ def run_ours(args) -> None:
     # end to end through the C ABI from pinned host memory
     e2e = None
     if not args.no_e2e:
-        host_in = [p["x"].cpu().pin_memory() for p in plans]
-        host_out = [torch.empty(p["y"].shape, dtype=torch.float32).pin_memory() for p in plans]
-        dev_in = [torch.empty_like(p["x"]) for p in plans]
-        ke = max(1, min(args.steps, 3))
-
-        def e2e_step():
-            for i, p in enumerate(plans):
-                with torch.cuda.stream(stream):
-                    dev_in[i].copy_(host_in[i], non_blocking=True)
-                check(p["hr"].exec_raw(dev_in[i].data_ptr(), p["spec"].data_ptr()), "exec r2c")
-                check(p["hc"].exec_raw(p["spec"].data_ptr(), p["y"].data_ptr()), "exec c2r")
-                with torch.cuda.stream(stream):
-                    host_out[i].copy_(p["y"], non_blocking=True)
-
-        e2e_step()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(ke):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e_ms = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
-        assert np.allclose(host_out[0][:2].numpy() / plans[0]["n"], host_in[0][:2].numpy(), atol=1e-5)
-        hb = sum(t.numel() * 4 for t in host_in)
-        db = sum(t.numel() * 4 for t in host_out)
-        e2e = {"value": round(world * step_flops / (e_ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
-               "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db,
-               "steps": ke}
+        e2e = run_e2e(torch, dev, plans, stream, max(1, min(args.steps, 3)), step_flops, world, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
