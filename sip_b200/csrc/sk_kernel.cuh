@@ -470,19 +470,33 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
     const bool sc = (a.flags & TF_SCALE) != 0;
     float2* dst = static_cast<float2*>(a.dst);
     if constexpr (K::OP == OP_R2C_HALF) {
-        constexpr int M = K::N, H = M + 1;
-        const int total = c.cnt * H;
+        // one thread per pair (k, M - k), k in [0, M/2]: Z[k], Z[M - k] and
+        // W_{2M}^k are read once; X[M - k] = conj(ev - W od) follows from
+        // W_{2M}^{M-k} = -conj(W_{2M}^k).  k = 0 also gives X[M].
+        constexpr int M = K::N, U = M / 2 + 1;
+        const int total = c.cnt * U;
         for (int f = tid; f < total; f += K::T) {
-            const int q = f / H;
-            const int k = f - q * H;
+            const int q = f / U;
+            const int k = f - q * U;
             const float2* row = buf + q * K::LD;
-            const float2 z = row[K::idx(k == M ? 0 : k)];
+            float2* out = dst + c.out_base + (long long)q * a.out_idist;
+            const float2 z = row[K::idx(k)];
             const float2 zm = row[K::idx(k == 0 ? 0 : M - k)];
             const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
             const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
-            float2 x = c_add(ev, c_mul(SIP_LDG(a.tw2 + k), od));
+            const float2 t = c_mul(SIP_LDG(a.tw2 + k), od);
+            float2 x = c_add(ev, t);
             if (sc) x = c_scale(x, a.scale);
-            dst[c.out_base + (long long)q * a.out_idist + k] = maybe_conj(x, cj);
+            out[k] = maybe_conj(x, cj);
+            if (k == 0) {  // X[M] = Re z0 - Im z0 (W_{2M}^M = -1)
+                float2 xm = make_float2(ev.x - t.x, ev.y - t.y);
+                if (sc) xm = c_scale(xm, a.scale);
+                out[M] = maybe_conj(xm, cj);
+            } else if (2 * k != M) {
+                float2 xm = make_float2(ev.x - t.x, t.y - ev.y);
+                if (sc) xm = c_scale(xm, a.scale);
+                out[M - k] = maybe_conj(xm, cj);
+            }
         }
     } else if constexpr (K::OP == OP_R2C_4B) {
         // rows k1 = i0 + q (slot q) and N1 - k1 (slot H + q) -> X[k1 + N1 k2]
