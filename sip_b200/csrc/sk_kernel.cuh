@@ -527,23 +527,27 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
             }
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
+        // one thread per bin k of a complex row: Z[k] and Z[N - k] give bin k
+        // of both real rows (x_a = Re part, x_b = Im part of the packed row)
         constexpr int N = K::N, H = N / 2 + 1;
         const int r0 = 2 * c.i0;
         const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
-        const int total = nrows * H;
+        const int total = ((nrows + 1) >> 1) * H;
         for (int f = tid; f < total; f += K::T) {
-            const int rl = f / H;
-            const int k = f - rl * H;
-            const float2* row = buf + (rl >> 1) * K::LD;
+            const int q = f / H;
+            const int k = f - q * H;
+            const float2* row = buf + q * K::LD;
             const float2 z = row[K::idx(k)];
             const float2 zm = row[K::idx(k == 0 ? 0 : N - k)];
-            float2 x;
-            if ((rl & 1) == 0)
-                x = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
-            else
-                x = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
-            if (sc) x = c_scale(x, a.scale);
-            dst[(long long)(r0 + rl) * a.out_idist + k] = maybe_conj(x, cj);
+            float2 xa = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            float2 xb = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            if (sc) {
+                xa = c_scale(xa, a.scale);
+                xb = c_scale(xb, a.scale);
+            }
+            const long long ra = r0 + 2 * q;
+            dst[ra * a.out_idist + k] = maybe_conj(xa, cj);
+            if (2 * q + 1 < nrows) dst[(ra + 1) * a.out_idist + k] = maybe_conj(xb, cj);
         }
     }
 }
