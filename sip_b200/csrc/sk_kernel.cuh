@@ -462,6 +462,23 @@ SIP_HD float2 sk_r2c_value(const TileArgs& a, float2 z, float2 zm, long long k) 
     return maybe_conj(x, (a.flags & TF_CONJ_OUT) != 0);
 }
 
+// X[k] and X[M - k] from Z[k], Z[M - k] with one twiddle: X[M - k] =
+// conj(ev - W od) since W_{2M}^{M-k} = -conj(W_{2M}^k).
+SIP_HD void sk_r2c_pair(const TileArgs& a, float2 z, float2 zm, long long k, float2* xk, float2* xmk) {
+    const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+    const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+    const float2 t = c_mul(cross_tw(a, k), od);
+    float2 x = c_add(ev, t);
+    float2 y = make_float2(ev.x - t.x, t.y - ev.y);
+    if (a.flags & TF_SCALE) {
+        x = c_scale(x, a.scale);
+        y = c_scale(y, a.scale);
+    }
+    const bool cj = (a.flags & TF_CONJ_OUT) != 0;
+    *xk = maybe_conj(x, cj);
+    *xmk = maybe_conj(y, cj);
+}
+
 // R2C post-process from the work layout (formulas of tile_io.cuh
 // store_r2c_half / store_r2c_pair), coalesced over the output rows.
 template <class K>
@@ -522,8 +539,7 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
                 x[kk] = sk_r2c_value(a, z, rq[K::idx(N2 - 1 - k2)], kk);
             } else {
                 const float2 zm = rm[K::idx(N2 - 1 - k2)];
-                x[kk] = sk_r2c_value(a, z, zm, kk);
-                x[M - kk] = sk_r2c_value(a, zm, z, M - kk);
+                sk_r2c_pair(a, z, zm, kk, x + kk, x + (M - kk));
             }
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
