@@ -298,6 +298,67 @@ def other_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> dict:
     return out
 
 
+# The reference's published device times (Ascend 950, CANN 9.2.0-beta.2;
+# tests/standalone/fft1d_optimized/REPORT_en.md:45-52,
+# example/Ascend950/FFT/fft-2d-c2c-4096x4096/README_en.md:61-62,
+# example/Ascend950/FFT/fft-2d-c2c-500x50/README_en.md:11,
+# docs/ops_fft_joint_build.md:29) for shapes this library runs as-is.
+PUBLISHED = [  # (name, type, direction, sizes, batch, reference microseconds)
+    ("c2c fwd 4096 x 4096", 0x10, 0x10, [4096], 4096, 234.790),
+    ("c2c inv 4096 x 4096", 0x10, 0x11, [4096], 4096, 234.044),
+    ("r2c fwd 4096 x 4096", 0x12, 0x10, [4096], 4096, 139.539),
+    ("c2r inv 4096 x 4096", 0x11, 0x11, [4096], 4096, 137.685),
+    ("c2c fwd 8192 x 8192", 0x10, 0x10, [8192], 8192, 1305.012),
+    ("r2c fwd 8192 x 8192", 0x12, 0x10, [8192], 8192, 544.499),
+    ("c2r inv 8192 x 8192", 0x11, 0x11, [8192], 8192, 533.636),
+    ("2d c2c fwd 4096^2", 0x10, 0x10, [4096, 4096], 1, 1590.0),
+    ("2d c2c fwd 500x50 x 12000", 0x10, 0x10, [500, 50], 12000, 5860.0),
+    ("c2c fwd 2^21 x 64", 0x10, 0x10, [1 << 21], 64, 53300.0),
+]
+
+
+def published_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> dict:
+    """The shapes the reference publishes device times for, timed the same
+    way (CUDA events, device-resident inputs, median-free mean of `steps`
+    execs), next to the published Ascend 950 time; not the same hardware."""
+    from sip_b200.fft import FftHandle, check
+
+    out = {}
+    for name, t, d, sizes, batch, ref_us in PUBLISHED:
+        last = sizes[-1]
+        lead = (batch,) + tuple(sizes[:-1])
+        if t == 0x10:
+            x = torch.randn(lead + (last,), dtype=torch.complex64, device=dev)
+            y = torch.empty_like(x)
+        elif t == 0x12:
+            x = torch.rand(lead + (last,), device=dev)
+            y = torch.empty(lead + (last // 2 + 1,), dtype=torch.complex64, device=dev)
+        else:
+            x = torch.randn(lead + (last // 2 + 1,), dtype=torch.complex64, device=dev)
+            y = torch.empty(lead + (last,), device=dev)
+        h = FftHandle()
+        if len(sizes) == 1:
+            check(h.make_plan_1d(sizes[0], t, d, batch), "plan")
+        else:
+            check(h.make_plan_2d(sizes[0], sizes[1], t, d, batch), "plan")
+        h.bind_workspace(dev)
+        check(h.set_stream(stream), "stream")
+        torch.cuda.synchronize()
+        for _ in range(warmup):
+            check(h.exec_raw(x.data_ptr(), y.data_ptr()), "exec")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            check(h.exec_raw(x.data_ptr(), y.data_ptr()), "exec")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) / steps * 1e3
+        out[name] = {"us": round(us, 2), "reference_us_ascend950": ref_us, "ratio": round(ref_us / us, 2)}
+        h.destroy()
+        del x, y
+    return out
+
+
 def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
     """Serving form: Poisson pulse-compression requests (N log-uniform over
     2,3,5-smooth lengths in [256, 2^18], batch uniform 1..512, delayed chirp
@@ -576,8 +637,10 @@ def run_ours(args) -> None:
     if rank == 0 and not args.no_precision:
         prec = precision_form(torch, dev, stream, steps=5, warmup=2)
     others = None
+    published = None
     if rank == 0 and not args.no_other:
         others = other_configs(torch, dev, stream)
+        published = published_configs(torch, dev, stream)
     serve = None
     if rank == 0 and not args.no_serve:
         serve = serving(torch, args.serve_requests)
@@ -605,6 +668,7 @@ def run_ours(args) -> None:
             "precision_form": prec,
             "serving": serve,
             "other_configs": others,
+            "reference_published_shapes": published,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,
         }

@@ -47,6 +47,19 @@
     X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 15, 8)          \
     X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 15, 8)           \
     X(3, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 1, 25, 15, 8)           \
+    /* real rows of N = 2048, 4096, 8192 (half lengths 1024, 2048, 4096) */  \
+    X(4, 1024, 4, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 4)          \
+    X(5, 1024, 4, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 4)           \
+    X(6, 2048, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 8)          \
+    X(7, 2048, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 8)           \
+    X(0, 4096, 1, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 16)         \
+    X(1, 4096, 1, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 16)          \
+    /* 2D 500 x 50 (the reference's MRI example shape): rows of 50, columns \
+       of 500 over the 50-wide slices */                                     \
+    X(2, 50, 16, 128, OP_C2C, SK_ROWS, -1, false, 2, 4, 1, 5, 10)                    \
+    X(3, 50, 16, 128, OP_C2C, SK_ROWS, 1, false, 2, 4, 1, 5, 10)                     \
+    X(4, 500, 10, 256, OP_C2C, SK_COLS, -1, false, 2, 2, 1, 25, 20)                  \
+    X(5, 500, 10, 256, OP_C2C, SK_COLS, 1, false, 2, 2, 1, 25, 20)                   \
     /* odd real length 2187 = 3^7, two rows per complex FFT */                \
     X(2, 2187, 2, 192, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 2, 1, 27, 9, 9)           \
     X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
