@@ -302,8 +302,30 @@ def other_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> dict:
 # tests/standalone/fft1d_optimized/REPORT_en.md:45-52,
 # example/Ascend950/FFT/fft-2d-c2c-4096x4096/README_en.md:61-62,
 # example/Ascend950/FFT/fft-2d-c2c-500x50/README_en.md:11,
-# docs/ops_fft_joint_build.md:29) for shapes this library runs as-is.
+# docs/ops_fft_joint_build.md:29, MULTIROW_REPORT_en.md:50-67, 81-86) for
+# shapes this library runs as-is.
 PUBLISHED = [  # (name, type, direction, sizes, batch, reference microseconds)
+    ("c2c fwd 1024 x 1024", 0x10, 0x10, [1024], 1024, 18.719),
+    ("c2c fwd 2048 x 2048", 0x10, 0x10, [2048], 2048, 64.930),
+    ("r2c fwd 2048 x 2048", 0x12, 0x10, [2048], 2048, 34.293),
+    ("c2c fwd 4096 x 8192", 0x10, 0x10, [4096], 8192, 406.776),
+    ("c2c fwd 544 x 8192", 0x10, 0x10, [544], 8192, 259.519),
+    ("c2c inv 2016 x 8192", 0x10, 0x11, [2016], 8192, 568.783),
+    ("c2c inv 2944 x 8192", 0x10, 0x11, [2944], 8192, 1362.876),
+    ("c2c inv 2976 x 8192", 0x10, 0x11, [2976], 8192, 1510.232),
+    ("c2c inv 3808 x 8192", 0x10, 0x11, [3808], 8192, 1600.467),
+    ("c2c fwd 3840 x 8192", 0x10, 0x10, [3840], 8192, 1096.466),
+    ("r2c fwd 5312 x 8192", 0x12, 0x10, [5312], 8192, 2479.435),
+    ("c2r inv 5344 x 8192", 0x11, 0x11, [5344], 8192, 4209.933),
+    ("r2c fwd 6688 x 8192", 0x12, 0x10, [6688], 8192, 2542.381),
+    ("c2r inv 6720 x 8192", 0x11, 0x11, [6720], 8192, 1508.922),
+    ("c2c fwd 6720 x 8192", 0x10, 0x10, [6720], 8192, 1789.091),
+    ("c2c inv 6752 x 8192", 0x10, 0x11, [6752], 8192, 10493.098),
+    ("c2c inv 8160 x 8192", 0x10, 0x11, [8160], 8192, 3735.701),
+    ("2d c2c fwd 544^2", 0x10, 0x10, [544, 544], 1, 53.796),
+    ("2d c2c inv 2016^2", 0x10, 0x11, [2016, 2016], 1, 333.939),
+    ("2d r2c fwd 1536^2", 0x12, 0x10, [1536, 1536], 1, 134.958),
+    ("2d c2r inv 1536^2", 0x11, 0x11, [1536, 1536], 1, 127.173),
     ("c2c fwd 4096 x 4096", 0x10, 0x10, [4096], 4096, 234.790),
     ("c2c inv 4096 x 4096", 0x10, 0x11, [4096], 4096, 234.044),
     ("r2c fwd 4096 x 4096", 0x12, 0x10, [4096], 4096, 139.539),
