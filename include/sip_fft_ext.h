@@ -51,7 +51,21 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
                                            C2R pre-process pass), 1 fuse both, 2 fuse neither */
 #define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant
                                            (0 default; a step without that variant uses its default) */
+#define SIP_FFT_HINT_RUNTIME_COMPILE 7  /* steps of a length without a compiled size-specialized
+                                           kernel: 0 default (compile one with NVRTC when the step
+                                           holds >= 2^20 values), 1 always, 2 never (generic kernel) */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
+
+/* Compiles (no GPU needed) the run-time specialized kernel the planner
+ * would choose for one tile step: op 0 C2C, 1 R2C half-length, 2 C2R
+ * half-length, 3 R2C row pairs, 4 C2R row pairs; mode 0 rows, 1 columns,
+ * 2 rows in / columns out; sign -1 or +1; tw4 1 for the four-step cross
+ * twiddle; n the tile transform length; transforms the step's count.
+ * ACL_SUCCESS when it compiled (or was in the cache), ACL_ERROR_API_NOT_SUPPORT
+ * when no run-time configuration fits or NVRTC is missing,
+ * ACL_ERROR_INTERNAL_ERROR when compilation failed.  No counterpart in the
+ * reference (a diagnostic of this library's run-time compiler).  */
+AsdSip::AspbStatus sipFftJitCompileCheck(int op, int mode, int sign, int tw4, int n, long long transforms);
 
 /* fftshift / ifftshift fused into the transform's output store (after
  * Create, before MakePlan; C2C 1-D and 2-D plans): mode 1 rotates every

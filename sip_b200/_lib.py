@@ -44,6 +44,7 @@ SIP_FFT_HINT_GENERIC_ONLY = 3
 SIP_FFT_HINT_RADIX_ORDER = 4
 SIP_FFT_HINT_REAL_FUSED = 5
 SIP_FFT_HINT_SK_VARIANT = 6
+SIP_FFT_HINT_RUNTIME_COMPILE = 7
 
 # Output shift modes (sipFftSetOutputShift).
 SIP_FFT_SHIFT_NONE = 0
@@ -72,6 +73,7 @@ EXPORTED = [
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
     "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows", "sipFftSetOutputShift",
+    "sipFftJitCompileCheck",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -116,6 +118,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftBatchUseGraphs": (_i32, [_vp, ctypes.c_int]),
         "sipFftBatchTakeStatus": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint)]),
         "sipFftExecC2CNoAlloc": (_i32, [_vp, _vp, _vp]),
+        "sipFftJitCompileCheck": (_i32, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_longlong]),
         "sipFftMakePlanPulse1D": (_i32, [_vp, _i64, _i64, _vp, ctypes.c_int]),
         "sipFftBatchAddRows": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
         "sipFftSetOutputShift": (_i32, [_vp, ctypes.c_int, ctypes.c_double]),

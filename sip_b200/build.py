@@ -46,7 +46,32 @@ UNITS = [
     ("device.cpp", [], "device.o"),
     ("api.cpp", [], "api.o"),
     ("acl_tensor.cpp", [], "acl_tensor.o"),
+    ("jit.cpp", [], "jit.o"),
+    (str(BUILD / "jit_headers.cpp"), [], "jit_headers.o"),
 ]
+
+# Kernel headers the run-time compiler (csrc/jit.cpp) builds sk kernels
+# from; embedded into the library so that it does not depend on the source
+# tree at run time.
+JIT_HEADERS = ["sk_kernel.cuh", "sk_modes.h", "fft_core.cuh", "tile_io.cuh"]
+
+
+def _gen_jit_headers() -> None:
+    BUILD.mkdir(exist_ok=True)
+    parts = ["// Generated by sip_b200/build.py: kernel headers for csrc/jit.cpp.", "namespace sipfft {",
+             f"extern const int kJitHeaderCount = {len(JIT_HEADERS)};",
+             "extern const char* const kJitHeaderNames[] = {" + ", ".join(f'"{h}"' for h in JIT_HEADERS) + "};",
+             "extern const char* const kJitHeaderTexts[] = {"]
+    for h in JIT_HEADERS:
+        text = (CSRC / h).read_text()
+        if ')sipjit"' in text:
+            raise RuntimeError(f"{h} contains the raw-string delimiter")
+        parts.append('R"sipjit(' + text + ')sipjit",')
+    parts += ["};", "}  // namespace sipfft", ""]
+    out = BUILD / "jit_headers.cpp"
+    new = "\n".join(parts)
+    if not out.exists() or out.read_text() != new:
+        out.write_text(new)
 
 
 def _newest_header() -> float:
@@ -56,7 +81,7 @@ def _newest_header() -> float:
 
 def _compile(src: str, defs: list[str], obj: str, head_mtime: float, verbose: bool) -> str:
     out = BUILD / obj
-    s = CSRC / src
+    s = CSRC / src  # an absolute src (generated under _build) replaces CSRC
     if out.exists() and out.stat().st_mtime >= max(s.stat().st_mtime, head_mtime):
         return f"up to date {obj}"
     cmd = [NVCC, *ARCH, *COMMON, *defs, "-c", str(s), "-o", str(out)]
@@ -70,6 +95,7 @@ def _compile(src: str, defs: list[str], obj: str, head_mtime: float, verbose: bo
 
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
+    _gen_jit_headers()
     head = _newest_header()
     jobs = jobs or max(1, os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -81,7 +107,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     objs = [str(BUILD / o) for _, _, o in UNITS]
     newest = max(Path(o).stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *objs]
+        cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *objs, "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -20,6 +20,7 @@
 
 #include "acl_tensor.h"
 #include "fft_api.h"
+#include "jit.h"
 #include "plan.h"
 #include "sip_fft_ext.h"
 #include "noalloc.h"
@@ -581,6 +582,20 @@ AspbStatus sipFftTakeDeviceErrors(unsigned* errors) {
     return sipfft::tc_take_error(errors) == cudaSuccess ? ACL_SUCCESS : ACL_ERROR_INTERNAL_ERROR;
 }
 
+AspbStatus sipFftJitCompileCheck(int op, int mode, int sign, int tw4, int n, long long transforms) {
+    sipfft::JitCfg c;
+    if (!sipfft::sk_jit_available() ||
+        !sipfft::sk_jit_choose(op, mode, sign, tw4 != 0, n, transforms, &c))
+        return ACL_ERROR_API_NOT_SUPPORT;
+    std::vector<char> cubin;
+    std::string lowered, err;
+    if (!sipfft::sk_jit_compile(c, &cubin, &lowered, &err)) {
+        std::fprintf(stderr, "sipFftJitCompileCheck: %s\n", err.c_str());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
 AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
     std::lock_guard<std::mutex> lk(g_mu);
     FftPlan* p = find_plan(handle);
@@ -609,6 +624,10 @@ AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
         case SIP_FFT_HINT_SK_VARIANT:
             if (value < 0 || value > 15) return ACL_ERROR_INVALID_PARAM;
             p->hint_sk_variant = value;
+            break;
+        case SIP_FFT_HINT_RUNTIME_COMPILE:
+            if (value < 0 || value > 2) return ACL_ERROR_INVALID_PARAM;
+            p->hint_jit = value;
             break;
         default:
             return ACL_ERROR_INVALID_PARAM;

@@ -11,6 +11,7 @@
 #include <sstream>
 #include <tuple>
 
+#include "jit.h"
 #include "plan.h"
 #include "tc_core.cuh"
 #include "tc_launch.h"
@@ -193,11 +194,14 @@ void prepare_device(FftPlan& plan) {
         st.L.args.tw2 = st.tw2 ? static_cast<const float2*>(st.tw2->ptr) : nullptr;
         if (st.sk != nullptr) {
             int per_sm = 1, sms = 1;
-            check(sk_prepare(st.sk->fn, st.L.smem_bytes, st.L.block, &per_sm), "sk_prepare");
+            // run-time specialized kernels are compiled (or fetched from the
+            // cache) on first use
+            const void* fn = st.sk->jit ? sk_jit_load(st.sk) : st.sk->fn;
+            check(sk_prepare(fn, st.L.smem_bytes, st.L.block, &per_sm), "sk_prepare");
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
             const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
             st.L.grid = (int)std::min<long long>(st.L.args.ntiles, resident);
-            st.L.sk_fn = st.sk->fn;
+            st.L.sk_fn = fn;
         } else {
             check(tile_prepare(st.L.sign, st.L.e, st.L.op, st.L.tw4, st.L.smem_bytes), "cudaFuncSetAttribute");
         }

@@ -18,8 +18,15 @@
 // natural order.
 #pragma once
 
+#if defined(__CUDACC_RTC__)
+// Runtime compilation (jit.cpp): the compiler provides the vector types.
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+typedef unsigned long long uintptr_t;
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #if defined(__CUDACC__)
 #define SIP_HD __host__ __device__ __forceinline__
@@ -402,7 +409,7 @@ constexpr int basis_count(int R) {
 
 // The radices a plan may use; every entry has a compiled pass.
 #define SIP_FFT_FOR_EACH_RADIX(X) \
-    X(2) X(3) X(4) X(5) X(7) X(8) X(9) X(10) X(11) X(13) X(15) X(16) X(17) X(19) X(25) X(27) X(32)
+    X(2) X(3) X(4) X(5) X(7) X(8) X(9) X(10) X(11) X(13) X(15) X(16) X(17) X(19) X(23) X(25) X(27) X(29) X(31) X(32)
 
 inline bool radix_supported(int r) {
     switch (r) {

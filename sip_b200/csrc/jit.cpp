@@ -1,0 +1,407 @@
+// Run-time specialization of the sk tile kernels (jit.h).
+#include "jit.h"
+
+#include <dlfcn.h>
+#include <nvrtc.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <fstream>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+#include "plan.h"
+#include "sk_kernel.cuh"
+
+namespace sipfft {
+
+// Kernel headers embedded by the build (generated jit_headers.cpp).
+extern const int kJitHeaderCount;
+extern const char* const kJitHeaderNames[];
+extern const char* const kJitHeaderTexts[];
+
+namespace {
+
+// ------------------------------------------------------------ NVRTC (dlopen)
+struct Nvrtc {
+    bool ok = false;
+    int major = 0, minor = 0;
+    nvrtcResult (*version)(int*, int*) = nullptr;
+    nvrtcResult (*create)(nvrtcProgram*, const char*, const char*, int, const char* const*,
+                          const char* const*) = nullptr;
+    nvrtcResult (*destroy)(nvrtcProgram*) = nullptr;
+    nvrtcResult (*add_name)(nvrtcProgram, const char*) = nullptr;
+    nvrtcResult (*compile)(nvrtcProgram, int, const char* const*) = nullptr;
+    nvrtcResult (*log_size)(nvrtcProgram, size_t*) = nullptr;
+    nvrtcResult (*log)(nvrtcProgram, char*) = nullptr;
+    nvrtcResult (*lowered)(nvrtcProgram, const char*, const char**) = nullptr;
+    nvrtcResult (*cubin_size)(nvrtcProgram, size_t*) = nullptr;
+    nvrtcResult (*cubin)(nvrtcProgram, char*) = nullptr;
+};
+
+const Nvrtc& nvrtc() {
+    static const Nvrtc api = [] {
+        Nvrtc a;
+        const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
+        void* h = nullptr;
+        for (const char* n : names)
+            if ((h = dlopen(n, RTLD_NOW | RTLD_LOCAL)) != nullptr) break;
+        if (h == nullptr) return a;
+        auto sym = [&](auto& fp, const char* name) {
+            fp = reinterpret_cast<std::remove_reference_t<decltype(fp)>>(dlsym(h, name));
+            return fp != nullptr;
+        };
+        a.ok = sym(a.version, "nvrtcVersion") && sym(a.create, "nvrtcCreateProgram") &&
+               sym(a.destroy, "nvrtcDestroyProgram") && sym(a.add_name, "nvrtcAddNameExpression") &&
+               sym(a.compile, "nvrtcCompileProgram") && sym(a.log_size, "nvrtcGetProgramLogSize") &&
+               sym(a.log, "nvrtcGetProgramLog") && sym(a.lowered, "nvrtcGetLoweredName") &&
+               sym(a.cubin_size, "nvrtcGetCUBINSize") && sym(a.cubin, "nvrtcGetCUBIN");
+        if (a.ok && a.version(&a.major, &a.minor) != NVRTC_SUCCESS) a.ok = false;
+        return a;
+    }();
+    return api;
+}
+
+// -default-device: the headers' unannotated constexpr helpers (evaluated at
+// compile time) are device functions here, as --expt-relaxed-constexpr
+// makes them usable for the library's nvcc build.
+const char* const kOptions[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-default-device"};
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return v != nullptr && *v ? std::atoi(v) : dflt;
+}
+
+// ------------------------------------------------------------ configuration
+// Cost of one pass of radix r in the run-time radix choice: passes
+// dominate (each is a shared-memory round trip), then larger radices and
+// the odd butterflies of the primes from 11 up.
+double jit_radix_cost(int r) {
+    int big = 1;
+    for (int p = 2, m = r; p <= m; ++p)
+        while (m % p == 0) {
+            big = p;
+            m /= p;
+        }
+    double c = 1.0 + 0.002 * r;
+    if (big >= 11) c += 0.2;
+    if (big >= 23) c += 0.3;
+    return c;
+}
+
+// Fewest, cheapest passes of radices 2..32 (any radix: the sk passes
+// build composite butterflies at compile time), largest first.
+std::vector<int> jit_radices(int n) {
+    std::map<int, std::pair<double, std::vector<int>>> memo;
+    std::function<std::pair<double, std::vector<int>>(int)> best = [&](int m) -> std::pair<double, std::vector<int>> {
+        if (m == 1) return {0.0, {}};
+        auto it = memo.find(m);
+        if (it != memo.end()) return it->second;
+        std::pair<double, std::vector<int>> res{1e30, {}};
+        for (int r = 32; r >= 2; --r) {
+            if (m % r != 0) continue;
+            auto sub = best(m / r);
+            if (sub.first >= 1e29) continue;
+            const double c = sub.first + jit_radix_cost(r);
+            if (c < res.first) {
+                res.first = c;
+                res.second = sub.second;
+                res.second.push_back(r);
+            }
+        }
+        memo[m] = res;
+        return res;
+    };
+    auto r = best(n);
+    if (r.first >= 1e29 || r.second.size() > (size_t)kMaxPasses) return {};
+    std::sort(r.second.begin(), r.second.end(), std::greater<int>());
+    return r.second;
+}
+
+// Threads so that no pass holds more than `e` values per thread (one
+// butterfly per thread for radices above e).
+int jit_threads(int P, int n, const std::vector<int>& radices, int e) {
+    long long t = 32;
+    for (int r : radices) {
+        const long long b = (long long)P * (n / r);
+        const long long per = std::max(1, e / r);
+        t = std::max(t, (b + per - 1) / per);
+    }
+    return (int)((t + 31) / 32 * 32);
+}
+
+// ------------------------------------------------------------ registry
+std::mutex g_jit_mu;
+std::deque<SkEntry> g_jit_entries;  // stable addresses
+std::map<std::string, SkEntry*> g_jit_index;
+std::map<std::string, const void*> g_jit_kernels;  // name expression -> loaded kernel
+
+JitCfg cfg_of(const SkEntry& e) {
+    JitCfg c;
+    c.op = e.op;
+    c.mode = e.mode;
+    c.sign = e.sign;
+    c.tw4 = e.tw4;
+    c.n = e.n;
+    c.P = e.P;
+    c.T = e.T;
+    c.stages = e.stages;
+    c.minb = e.minb;
+    c.radices = e.radices;
+    c.LD = e.LD;
+    c.smem = e.smem;
+    return c;
+}
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= b[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+std::string cache_dir() {
+    const char* env = std::getenv("SIP_FFT_JIT_CACHE");
+    std::string d;
+    if (env != nullptr) {
+        d = env;
+    } else {
+        const char* home = std::getenv("HOME");
+        if (home == nullptr || *home == 0) return "";
+        d = std::string(home) + "/.cache/sip_fft_jit";
+    }
+    // mkdir -p
+    for (size_t i = 1; i <= d.size(); ++i)
+        if (i == d.size() || d[i] == '/') mkdir(d.substr(0, i).c_str(), 0755);
+    struct stat st {};
+    if (stat(d.c_str(), &st) != 0 || !S_ISDIR(st.st_mode)) return "";
+    return d;
+}
+
+// Cache file: "SIPJIT1\n<lowered name>\n<cubin bytes>".
+bool cache_read(const std::string& path, std::vector<char>* cubin, std::string* lowered) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    std::string magic;
+    if (!std::getline(f, magic) || magic != "SIPJIT1") return false;
+    if (!std::getline(f, *lowered) || lowered->empty()) return false;
+    cubin->assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    return !cubin->empty();
+}
+
+void cache_write(const std::string& path, const std::vector<char>& cubin, const std::string& lowered) {
+    const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
+    {
+        std::ofstream f(tmp, std::ios::binary);
+        if (!f) return;
+        f << "SIPJIT1\n" << lowered << "\n";
+        f.write(cubin.data(), (std::streamsize)cubin.size());
+        if (!f) {
+            std::remove(tmp.c_str());
+            return;
+        }
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
+
+}  // namespace
+
+bool sk_jit_available() {
+    const char* env = std::getenv("SIP_FFT_JIT");
+    if (env != nullptr && std::strcmp(env, "0") == 0) return false;
+    return nvrtc().ok;
+}
+
+bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out) {
+    const bool row_op = op == OP_R2C_HALF || op == OP_C2R_HALF || op == OP_R2C_PAIR || op == OP_C2R_PAIR;
+    if (op != OP_C2C && !row_op) return false;
+    if (row_op && (mode != SK_ROWS || tw4)) return false;
+    if ((op == OP_R2C_PAIR || op == OP_C2R_PAIR) && n % 2 == 0) return false;
+    if (n < 8 || n > kMaxTileN) return false;
+    JitCfg c;
+    c.op = op;
+    c.mode = mode;
+    c.sign = sign;
+    c.tw4 = tw4;
+    c.n = n;
+    c.radices = jit_radices(n);
+    if (c.radices.empty()) return false;
+    transforms = std::max<long long>(1, transforms);
+    // transforms per tile: about SIP_FFT_JIT_TILE (4096) values for rows,
+    // runs of 16 adjacent transforms (128-byte segments) for the column
+    // modes; at most SIP_FFT_JIT_E (32) values per thread and pass
+    const int tile_values = std::max(64, env_int("SIP_FFT_JIT_TILE", 4096));
+    const int per_thread = std::max(8, env_int("SIP_FFT_JIT_E", 32));
+    long long P = mode == SK_ROWS ? std::max(1, tile_values / n) : 16;
+    P = std::min<long long>(P, transforms);
+    int T = 0;
+    for (;;) {
+        T = jit_threads((int)P, n, c.radices, per_thread);
+        if (T > kMaxTileThreads && P == 1) T = jit_threads(1, n, c.radices, 2 * per_thread);
+        if (T <= kMaxTileThreads || P == 1) break;
+        P = std::max<long long>(1, P / 2);
+    }
+    if (T > kMaxTileThreads) return false;
+    c.P = (int)P;
+    c.T = T;
+    const int r0 = c.radices[0];
+    c.LD = sk_pitch(n, r0);
+    const long long buf = (long long)sk_buffer_values(op, c.P, n, r0) * 8;
+    if (2 * buf <= kMaxTileSmem) c.stages = 2;
+    else if (buf <= kMaxTileSmem) c.stages = 1;
+    else return false;
+    c.smem = (int)(c.stages * buf);
+    const int smem_ctas = std::max<int>(1, (228 * 1024) / (c.smem + 1024));
+    c.minb = std::max(1, std::min(65536 / (T * 128), smem_ctas));
+    *out = c;
+    return true;
+}
+
+std::string sk_jit_source() { return "#include \"sk_kernel.cuh\"\n"; }
+
+std::string sk_jit_name_expr(const JitCfg& c) {
+    std::ostringstream s;
+    s << "&sipfft::sk_fft_kernel<sipfft::SkCfg<" << c.n << ", " << c.P << ", " << c.T << ", " << c.op << ", "
+      << c.mode << ", " << c.sign << ", " << (c.tw4 ? "true" : "false") << ", " << c.minb << ", 1";
+    for (int r : c.radices) s << ", " << r;
+    s << ">, " << c.stages << ">";
+    return s.str();
+}
+
+bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err) {
+    const Nvrtc& api = nvrtc();
+    if (!api.ok) {
+        *err = "NVRTC is not available";
+        return false;
+    }
+    const std::string src = sk_jit_source();
+    const std::string expr = sk_jit_name_expr(c);
+    uint64_t h = 1469598103934665603ull;
+    const int ver[2] = {api.major, api.minor};
+    h = fnv1a(h, ver, sizeof(ver));
+    for (const char* o : kOptions) h = fnv1a(h, o, std::strlen(o) + 1);
+    h = fnv1a(h, src.data(), src.size());
+    h = fnv1a(h, expr.data(), expr.size());
+    for (int i = 0; i < kJitHeaderCount; ++i) {
+        h = fnv1a(h, kJitHeaderNames[i], std::strlen(kJitHeaderNames[i]) + 1);
+        h = fnv1a(h, kJitHeaderTexts[i], std::strlen(kJitHeaderTexts[i]) + 1);
+    }
+    char hex[17];
+    std::snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
+    const std::string dir = cache_dir();
+    const std::string path = dir.empty() ? "" : dir + "/sk_" + hex + ".cubin";
+    if (!path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(path, cubin, lowered)) return true;
+
+    nvrtcProgram prog = nullptr;
+    if (api.create(&prog, src.c_str(), "sip_fft_jit.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
+        NVRTC_SUCCESS) {
+        *err = "nvrtcCreateProgram failed";
+        return false;
+    }
+    // SIP_FFT_JIT_VERBOSE=1 prints the compiler's resource report (registers,
+    // spills) of every kernel compiled here
+    const bool verbose = env_int("SIP_FFT_JIT_VERBOSE", 0) != 0;
+    std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
+    if (verbose) opts.push_back("--ptxas-options=-v");
+    bool ok = api.add_name(prog, expr.c_str()) == NVRTC_SUCCESS;
+    const nvrtcResult rc = ok ? api.compile(prog, (int)opts.size(), opts.data()) : NVRTC_ERROR_INVALID_INPUT;
+    size_t ls = 0;
+    std::string log;
+    if (api.log_size(prog, &ls) == NVRTC_SUCCESS && ls > 1) {
+        log.resize(ls);
+        api.log(prog, &log[0]);
+    }
+    if (verbose) std::fprintf(stderr, "sip_fft jit %s\n%s\n", expr.c_str(), log.c_str());
+    if (rc != NVRTC_SUCCESS) {
+        *err = "NVRTC failed for " + expr + ": " + log.substr(0, 2000);
+        api.destroy(&prog);
+        return false;
+    }
+    const char* low = nullptr;
+    size_t cs = 0;
+    ok = api.lowered(prog, expr.c_str(), &low) == NVRTC_SUCCESS && low != nullptr &&
+         api.cubin_size(prog, &cs) == NVRTC_SUCCESS && cs > 0;
+    if (ok) {
+        *lowered = low;
+        cubin->resize(cs);
+        ok = api.cubin(prog, cubin->data()) == NVRTC_SUCCESS;
+    }
+    api.destroy(&prog);
+    if (!ok) {
+        *err = "NVRTC produced no kernel for " + expr;
+        return false;
+    }
+    if (!path.empty()) cache_write(path, *cubin, *lowered);
+    return true;
+}
+
+const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms) {
+    if (!sk_jit_available()) return nullptr;
+    JitCfg c;
+    if (!sk_jit_choose(op, mode, sign, tw4, n, transforms, &c)) return nullptr;
+    const std::string key = sk_jit_name_expr(c);
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    auto it = g_jit_index.find(key);
+    if (it != g_jit_index.end()) return it->second;
+    SkEntry e;
+    e.n = n;
+    e.P = c.P;
+    e.T = c.T;
+    e.op = op;
+    e.mode = mode;
+    e.sign = sign;
+    e.tw4 = tw4;
+    e.twb = true;
+    e.stages = c.stages;
+    e.radices = c.radices;
+    e.LD = c.LD;
+    e.smem = c.smem;
+    e.fn = nullptr;
+    e.minb = c.minb;
+    e.jit = true;
+    auto kit = g_jit_kernels.find(key);
+    if (kit != g_jit_kernels.end()) e.fn = kit->second;
+    g_jit_entries.push_back(e);
+    g_jit_index[key] = &g_jit_entries.back();
+    return &g_jit_entries.back();
+}
+
+const void* sk_jit_load(const SkEntry* entry) {
+    const JitCfg c = cfg_of(*entry);
+    const std::string key = sk_jit_name_expr(c);
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        auto kit = g_jit_kernels.find(key);
+        if (kit != g_jit_kernels.end()) return kit->second;
+    }
+    std::vector<char> cubin;
+    std::string lowered, err;
+    if (!sk_jit_compile(c, &cubin, &lowered, &err)) throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, err);
+    cudaLibrary_t lib = nullptr;
+    cudaError_t e = cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e != cudaSuccess)
+        throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e));
+    cudaKernel_t k = nullptr;
+    e = cudaLibraryGetKernel(&k, lib, lowered.c_str());
+    if (e != cudaSuccess)
+        throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, std::string("cudaLibraryGetKernel: ") + cudaGetErrorString(e));
+    const void* fn = reinterpret_cast<const void*>(k);
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    auto kit = g_jit_kernels.find(key);
+    if (kit != g_jit_kernels.end()) return kit->second;  // another thread loaded it first; lib stays loaded
+    g_jit_kernels[key] = fn;
+    auto it = g_jit_index.find(key);
+    if (it != g_jit_index.end()) it->second->fn = fn;
+    return fn;
+}
+
+}  // namespace sipfft

@@ -1,0 +1,50 @@
+// Run-time specialization of the size-specialized tile kernels.
+//
+// sk_configs.h compiles sk kernels for a fixed list of lengths; every other
+// length would run on the generic tile kernel, whose pass loop dispatches
+// on the radix at run time.  For those lengths the planner can instead
+// pick an sk configuration here (radices, transforms per tile, threads,
+// stages, register target) and have NVRTC compile sk_fft_kernel<that
+// configuration> from the library's own kernel headers, embedded in the
+// library at build time.  Compilation happens once per configuration and
+// process, when a plan that uses it is first prepared on a device, and the
+// cubin is kept in an on-disk cache (SIP_FFT_JIT_CACHE, default
+// $HOME/.cache/sip_fft_jit) keyed by a hash of the source, the headers, the
+// options and the NVRTC version.  NVRTC is loaded with dlopen; without it
+// no run-time entry is offered and the generic kernel runs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "sk_registry.h"
+
+namespace sipfft {
+
+struct JitCfg {
+    int op = 0, mode = 0, sign = -1;
+    bool tw4 = false;
+    int n = 0, P = 1, T = 32, stages = 2, minb = 1;
+    std::vector<int> radices;
+    int LD = 0, smem = 0;
+};
+
+// Host-side choice of a configuration (no CUDA or NVRTC calls).
+bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out);
+
+// The NVRTC source and the kernel's name expression for a configuration.
+std::string sk_jit_source();
+std::string sk_jit_name_expr(const JitCfg& c);
+
+// Compiles a configuration to a cubin (through the disk cache); returns
+// false with the compiler log in *err on failure.
+bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err);
+
+// Compiles and loads the kernel of a run-time entry (from sk_jit_entry)
+// and stores it in the entry; returns the kernel.  Throws PlanError when
+// compilation or loading fails.
+const void* sk_jit_load(const SkEntry* e);
+
+}  // namespace sipfft

@@ -46,7 +46,7 @@ int64_t FftPlan::elements() const {
 namespace {
 thread_local int g_compute_mode = kComputeFp32;
 thread_local int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0,
-                 g_hint_variant = 0;
+                 g_hint_variant = 0, g_hint_jit = 0;
 }  // namespace
 
 // ------------------------------------------------------------ radices
@@ -63,16 +63,17 @@ struct RadixCost {
 double radix_cost(int r) {
     double c = 1.0 + 0.002 * r;
     if (r == 11 || r == 13 || r == 17 || r == 19) c += 0.2;
+    if (r == 23 || r == 29 || r == 31) c += 0.5;
     return c;
 }
 
-const int kRadixList[] = {32, 27, 25, 19, 17, 16, 15, 13, 11, 10, 9, 8, 7, 5, 4, 3, 2};
+const int kRadixList[] = {32, 31, 29, 27, 25, 23, 19, 17, 16, 15, 13, 11, 10, 9, 8, 7, 5, 4, 3, 2};
 
 }  // namespace
 
 std::vector<int> choose_radices(int n, int e) {
     if (n == 1) return {};
-    const int maxr = e >= 32 ? 32 : 27;
+    const int maxr = e >= 32 ? 32 : 31;  // a pass needs R < 2E
     std::map<int, std::pair<double, std::vector<int>>> memo;
     std::function<std::pair<double, std::vector<int>>(int)> best = [&](int m) -> std::pair<double, std::vector<int>> {
         if (m == 1) return {0.0, {}};
@@ -203,6 +204,11 @@ void try_specialize(Step& st, const AxisIO& io) {
     const int mode = sk_mode_of(L.op, a.N, io);
     if (mode < 0) return;
     const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
+    // No compiled kernel for this length: a run-time compiled one (jit.cpp)
+    // for steps large enough to repay the compilation, or on request.
+    const long long values = io.inner * io.outer * (long long)a.N;
+    if (e == nullptr && (g_hint_jit == 1 || (g_hint_jit == 0 && values >= (1LL << 20))))
+        e = sk_jit_entry(L.op, mode, L.sign, L.tw4, a.N, io.inner);
     if (e == nullptr) return;
     st.sk = e;
     st.radices = e->radices;
@@ -217,7 +223,7 @@ void try_specialize(Step& st, const AxisIO& io) {
     a.div_p = make_fastdiv((uint32_t)e->P);
     a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
     L.grid = a.ntiles;  // capped to the resident CTAs at device preparation
-    st.what += " [sk P=" + std::to_string(e->P) + "]";
+    st.what += std::string(e->jit ? " [sk jit P=" : " [sk P=") + std::to_string(e->P) + "]";
 }
 
 
@@ -840,11 +846,11 @@ bool apply_tune_cache(FftPlan& plan) {
     char line[512];
     bool hit = false;
     while (std::fgets(line, sizeof(line), f)) {
-        int type = 0, dir = 0, p = 0, e = 0, gen = 0, order = 0, fused = 0, variant = 0;
+        int type = 0, dir = 0, p = 0, e = 0, gen = 0, order = 0, fused = 0, variant = 0, jit = 0;
         long long batch = 0;
         char d[256] = {0};
-        const int got = std::sscanf(line, "%d %d %255s %lld %d %d %d %d %d %d", &type, &dir, d, &batch, &p, &e, &gen,
-                                    &order, &fused, &variant);
+        const int got = std::sscanf(line, "%d %d %255s %lld %d %d %d %d %d %d %d", &type, &dir, d, &batch, &p, &e,
+                                    &gen, &order, &fused, &variant, &jit);
         if (got < 8) continue;
         if (type == (int)plan.type && dir == (int)plan.direction && dims == d && batch == plan.batch) {
             plan.hint_p = p;
@@ -853,6 +859,7 @@ bool apply_tune_cache(FftPlan& plan) {
             plan.hint_order = order;
             plan.hint_real_fused = got >= 9 ? fused : 0;
             plan.hint_sk_variant = got >= 10 ? variant : 0;
+            plan.hint_jit = got >= 11 ? jit : 0;
             hit = true;  // the last matching line wins
         }
     }
@@ -868,6 +875,7 @@ void build_steps(FftPlan& plan) {
     g_hint_order = plan.hint_order;
     g_hint_real_fused = plan.hint_real_fused;
     g_hint_variant = plan.hint_sk_variant;
+    g_hint_jit = plan.hint_jit;
     plan.steps.clear();
     plan.workspace_need = 0;
     if (plan.pulse) {
@@ -987,7 +995,7 @@ std::string describe(const FftPlan& plan) {
                << ",\"flags\":" << a.flags << ",\"inner\":" << a.inner << ",\"tiles_per_outer\":" << a.tiles_per_outer
                << ",\"in\":[" << a.in_odist << "," << a.in_idist << "," << a.in_stride << "],\"out\":["
                << a.out_odist << "," << a.out_idist << "," << a.out_stride << "],\"sk\":" << (st.sk ? "true" : "false")
-               << ",\"radices\":[";
+               << ",\"jit\":" << (st.sk && st.sk->jit ? "true" : "false") << ",\"radices\":[";
             for (size_t r = 0; r < st.radices.size(); ++r) os << (r ? "," : "") << st.radices[r];
             os << "]";
         } else if (st.kind == StepKind::Blue) {

@@ -88,6 +88,7 @@ struct FftPlan {
     int hint_order = 0;    // radix order: 0 descending, 1 ascending
     int hint_real_fused = 0;  // real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
     int hint_sk_variant = 0;  // which compiled size-specialized variant (sk_configs.h order)
+    int hint_jit = 0;  // run-time compiled sk kernels: 0 default (large steps), 1 always, 2 never
     bool hints_explicit = false;
     // Pulse-compression plan (sipFftMakePlanPulse1D): x -> IFFT(FFT(x) * F)
     // per row, F a device spectrum of length sizes[0] owned by the caller.

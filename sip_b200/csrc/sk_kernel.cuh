@@ -21,10 +21,34 @@
 #pragma once
 
 #include "fft_core.cuh"
-#include "sk_registry.h"
+#include "sk_modes.h"
 #include "tile_io.cuh"
 
 namespace sipfft {
+
+// Tile layout of a configuration as plain functions of its parameters, so
+// that the runtime compiler's host side (jit.cpp) sizes a tile exactly as
+// SkCfg does.  Odd first radices write conflict-free unpadded; even ones
+// need a pad slot every max(16, R0) values (radix-32 strides need one per 32).
+SIP_HD constexpr int sk_pad_group(int r0) { return r0 > 16 ? r0 : 16; }
+SIP_HD constexpr int sk_index(int n, int r0) { return r0 % 2 == 0 ? n + n / sk_pad_group(r0) : n; }
+// Work-layout pitch: element n of transform q at q * LD + sk_index(n), LD odd.
+SIP_HD constexpr int sk_pitch(int n, int r0) {
+    return ((sk_index(n - 1, r0) + 1) & 1) ? sk_index(n - 1, r0) + 1 : sk_index(n - 1, r0) + 2;
+}
+// Staged input values (complex64 units) per tile.
+SIP_HD constexpr int sk_stage_values(int op, int p, int n) {
+    return op == OP_C2R_HALF ? p * (n + 1)
+         : (op == OP_R2C_4B || op == OP_C2R_4A) ? p * n
+         : op == OP_C2R_PAIR ? p * (n + 1)
+         : p * n;  // R2C pair: 2P rows of N floats = P*N complex slots
+}
+// Complex values per buffer, rounded up to an even count so that the
+// second buffer starts on a 16-byte boundary (cp.async 16-byte copies).
+SIP_HD constexpr int sk_buffer_values(int op, int p, int n, int r0) {
+    return ((sk_stage_values(op, p, n) > p * sk_pitch(n, r0) ? sk_stage_values(op, p, n) : p * sk_pitch(n, r0)) + 1) /
+           2 * 2;
+}
 
 template <int N_, int P_, int T_, int OP_, int MODE_, int SIGN_, bool TW4_, int MINB_, int TWB_, int... Rs>
 struct SkCfg {
@@ -58,11 +82,7 @@ struct SkCfg {
         return off;
     }
     static constexpr int tw_entries() { return twoff(NP); }
-    // Odd first radices write conflict-free unpadded; even ones need a pad
-    // slot every max(16, R0) values (radix-32 strides need one per 32).
-    static constexpr bool PAD = radix(0) % 2 == 0;
-    static constexpr int PADG = radix(0) > 16 ? radix(0) : 16;
-    static constexpr int idx(int n) { return PAD ? n + n / PADG : n; }
+    static constexpr int idx(int n) { return sk_index(n, radix(0)); }
     static constexpr bool colmap(int p) {
         return MODE == SK_COLS || (MODE == SK_ROWS_T && p == NP - 1 && OP == OP_C2C);
     }
@@ -72,16 +92,9 @@ struct SkCfg {
     static constexpr int H = P / 2;
     static constexpr int slots(int p) { return (P * (N / radix(p)) + T - 1) / T; }
 
-    // Work layout: element n of transform q at q * LD + idx(n), LD odd.
-    static constexpr int LD = ((idx(N - 1) + 1) & 1) ? idx(N - 1) + 1 : idx(N - 1) + 2;
-    // Staged input values (complex64 units) per tile.
-    static constexpr int STAGE = OP == OP_C2R_HALF ? P * (N + 1)
-                               : (OP == OP_R2C_4B || OP == OP_C2R_4A) ? P * N
-                               : OP == OP_C2R_PAIR ? P * (N + 1)
-                               : P * N;  // R2C pair: 2P rows of N floats = P*N complex slots
-    // Complex values per buffer, rounded up to an even count so that the
-    // second buffer starts on a 16-byte boundary (cp.async 16-byte copies).
-    static constexpr int BUF = ((STAGE > P * LD ? STAGE : P * LD) + 1) / 2 * 2;
+    static constexpr int LD = sk_pitch(N, radix(0));
+    static constexpr int STAGE = sk_stage_values(OP, P, N);
+    static constexpr int BUF = sk_buffer_values(OP, P, N, radix(0));
     static constexpr int SMEM = 2 * BUF * 8;
     // CTAs per SM the shared memory allows with two stages (228 KB per SM,
     // 1 KB reserved per CTA); used as the register-allocation target.

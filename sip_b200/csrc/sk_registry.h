@@ -3,13 +3,9 @@
 
 #include <vector>
 
-namespace sipfft {
+#include "sk_modes.h"
 
-enum SkMode : int {
-    SK_ROWS = 0,    // transforms are contiguous rows; the tile is one contiguous run
-    SK_COLS = 1,    // transforms are adjacent columns (in_idist = out_idist = 1)
-    SK_ROWS_T = 2,  // contiguous rows in, adjacent columns out (four-step pass B)
-};
+namespace sipfft {
 
 struct SkEntry {
     int n, P, T, op, mode, sign;
@@ -21,6 +17,8 @@ struct SkEntry {
     int smem;        // dynamic shared memory per CTA (bytes)
     const void* fn;  // kernel (library) or CPU runner (test harness)
     int order = 0;   // position in the SIP_SK_CONFIGS list
+    int minb = 0;    // CTAs-per-SM register target (__launch_bounds__)
+    bool jit = false;  // compiled at run time (jit.cpp); fn is set by sk_jit_load
 };
 
 // The `variant`-th entry compiled for (op, mode, sign, tw4, n) in
@@ -29,5 +27,12 @@ struct SkEntry {
 const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant = 0);
 
 const std::vector<SkEntry>& sk_registry();
+
+// Run-time specialization (jit.cpp): an entry for a configuration that
+// sk_configs.h does not compile, chosen from (op, mode, n, transforms);
+// its kernel is compiled by NVRTC when the plan is first prepared on a
+// device.  nullptr when no configuration fits or NVRTC is not available.
+const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms);
+bool sk_jit_available();
 
 }  // namespace sipfft

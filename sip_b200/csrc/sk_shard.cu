@@ -29,6 +29,7 @@ SkEntry make_entry(std::vector<int> radices) {
     e.LD = K::LD;
     e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8;
     e.fn = reinterpret_cast<const void*>(&sk_fft_kernel<K, STAGES>);
+    e.minb = K::MINB;
     return e;
 }
 

@@ -57,7 +57,8 @@ def test_ref_c2c_3d(emu, x, y, z, batch, direction):
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 @pytest.mark.parametrize("sizes,batch", [([1], 3), ([2], 5), ([3], 4), ([7], 3), ([1000], 5), ([2187], 3),
                                          ([6000], 2), ([65536], 1), ([40000], 1), ([8, 8], 3), ([30, 33], 3),
-                                         ([9, 7, 5], 2), ([1, 12], 2), ([5, 1, 4], 1)])
+                                         ([9, 7, 5], 2), ([1, 12], 2), ([5, 1, 4], 1),
+                                         ([2944], 2), ([2976], 2), ([1856], 2), ([667], 3), ([961], 2)])
 def test_plan_kinds(emu, op, direction, sizes, batch):
     x = random_input(op, sizes, batch, seed=sum(sizes) + batch)
     _check(emu, op, direction, sizes, batch, x)

@@ -29,7 +29,8 @@ def test_bluestein_harness(emu, n, op, direction):
     assert err <= REL_L2_TOL, err
 
 
-def test_direct_lengths_do_not_use_bluestein(emu):
-    x = random_input(O.C2C, [1000], 2)
-    rc, _, desc = emu_run(emu, O.C2C, O.FORWARD, [1000], 2, x)
+@pytest.mark.parametrize("n", [1000, 2944, 2976, 1856])  # 2^7 23, 2^5 3 31, 2^6 29 have prime radix passes
+def test_direct_lengths_do_not_use_bluestein(emu, n):
+    x = random_input(O.C2C, [n], 2)
+    rc, _, desc = emu_run(emu, O.C2C, O.FORWARD, [n], 2, x)
     assert rc == 0 and "bluestein" not in desc

@@ -137,9 +137,29 @@ def test_large_real_forms(cuda, op, direction, fused):
     h.destroy()
 
 
+# Lengths whose factors include the prime radices 23, 29 and 31, planned
+# as direct passes: 2^7 23, 2^5 3 31, 2^6 29, 31^2, 23 29, and 23 31 29 2^2
+# above one tile.
+@pytest.mark.parametrize("n,batch", [(2944, 40), (2976, 40), (1856, 33), (961, 17), (667, 9), (82708, 3)])
+@pytest.mark.parametrize("op", [O.C2C, O.R2C, O.C2R])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_prime_radix_lengths(cuda, n, batch, op, direction):
+    rng = np.random.default_rng(n + 7 * op)
+    ishape, idt, _, _ = shapes(op, [n], batch)
+    if op == O.C2R:
+        x = np.fft.rfft(rng.uniform(-1, 1, (batch, n))).astype(np.complex64)
+    elif idt == np.float32:
+        x = rng.uniform(-1, 1, ishape).astype(np.float32)
+    else:
+        x = (rng.standard_normal(ishape) + 1j * rng.standard_normal(ishape)).astype(np.complex64)
+    out = gpu_run(cuda, op, direction, [n], batch, x)
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+
+
 # Lengths with a prime factor above 32: Bluestein (pre pass, fused
 # convolution of a 2,3,5-smooth length, post pass).
-@pytest.mark.parametrize("n,batch", [(31, 5), (37, 64), (1009, 33), (4099, 7), (2 * 8191, 5), (20011, 3),
+@pytest.mark.parametrize("n,batch", [(41, 5), (37, 64), (1009, 33), (4099, 7), (2 * 8191, 5), (20011, 3),
                                      (65537, 2)])
 @pytest.mark.parametrize("op", [O.C2C, O.R2C, O.C2R])
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])

@@ -1,0 +1,166 @@
+"""Run-time specialized tile kernels (csrc/jit.cpp).
+
+Lengths without a compiled size-specialized kernel get one compiled by
+NVRTC from the library's own kernel headers.  CPU tests: the planner's
+choice (describe) and that the generated source compiles for every tile
+mode and real-transform operation (NVRTC needs no GPU).  GPU tests: parity
+of the compiled kernels with the FP64 oracle, forced on at small batches
+with SIP_FFT_HINT_RUNTIME_COMPILE = 1, against the generic kernel too.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sip_b200 import _lib as L
+from tests.fftcase import settle, shapes
+
+REL_L2_TOL = 1e-6
+
+OP_C2C, OP_R2C_HALF, OP_C2R_HALF, OP_R2C_PAIR, OP_C2R_PAIR = 0, 1, 2, 3, 4
+ROWS, COLS, ROWS_T = 0, 1, 2
+
+
+@pytest.fixture()
+def jit_cache(tmp_path, monkeypatch):
+    monkeypatch.setenv("SIP_FFT_JIT_CACHE", str(tmp_path / "jit"))
+    return tmp_path / "jit"
+
+
+def _plan(op, direction, sizes, batch, jit):
+    from sip_b200.fft import FftHandle, check
+
+    h = FftHandle()
+    check(h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, jit), "hint")
+    rc = {1: lambda: h.make_plan_1d(sizes[0], op, direction, batch),
+          2: lambda: h.make_plan_2d(sizes[0], sizes[1], op, direction, batch)}[len(sizes)]()
+    check(rc, "make plan")
+    return h
+
+
+def _nvrtc_present():
+    return L.lib().sipFftJitCompileCheck(OP_C2C, ROWS, -1, 0, 3840, 64) != L.ACL_ERROR_API_NOT_SUPPORT
+
+
+@pytest.mark.parametrize("op,direction,n,batch,jit,expect", [
+    (O.C2C, O.FORWARD, 3840, 8192, 0, True),    # 31M values: compiled at run time by default
+    (O.C2C, O.FORWARD, 3840, 16, 0, False),     # small step: generic kernel
+    (O.C2C, O.FORWARD, 3840, 16, 1, True),      # forced on
+    (O.C2C, O.FORWARD, 3840, 8192, 2, False),   # forced off
+    (O.C2C, O.FORWARD, 4096, 8192, 1, False),   # a compiled kernel exists: no run-time one
+    (O.R2C, O.FORWARD, 6688, 8, 1, True),
+    (O.C2R, O.INVERSE, 2001, 8, 1, True),       # odd real length: row pairs
+])
+def test_planner_choice(op, direction, n, batch, jit, expect):
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    h = _plan(op, direction, [n], batch, jit)
+    steps = [s for s in h.describe()["steps"] if "jit" in s]
+    h.destroy()
+    assert any(s["jit"] for s in steps) == expect, steps
+    for s in steps:
+        if s["jit"]:
+            assert s["sk"] and 32 <= s["threads"] <= 512 and s["threads"] % 32 == 0
+            assert int(np.prod(s["radices"])) == s["n"] and max(s["radices"]) <= 32
+
+
+def test_hint_validation():
+    from sip_b200.fft import FftHandle
+
+    h = FftHandle()
+    assert h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, 3) == L.ACL_ERROR_INVALID_PARAM
+    assert h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, 2) == L.ACL_SUCCESS
+    h.destroy()
+
+
+# One configuration per operation and tile mode (compiled on the CPU).
+COMPILE_CASES = [
+    (OP_C2C, ROWS, -1, 0, 3840, 8192),
+    (OP_C2C, ROWS, 1, 0, 2944, 8192),       # radix 23
+    (OP_C2C, COLS, -1, 1, 243, 9000),       # four-step column pass with cross twiddles
+    (OP_C2C, ROWS_T, 1, 0, 625, 9000),      # four-step row pass, transposed store
+    (OP_R2C_HALF, ROWS, -1, 0, 3344, 8192),
+    (OP_C2R_HALF, ROWS, 1, 0, 3344, 8192),
+    (OP_R2C_PAIR, ROWS, -1, 0, 2001, 1000),
+    (OP_C2R_PAIR, ROWS, 1, 0, 2001, 1000),
+]
+
+
+@pytest.mark.parametrize("op,mode,sign,tw4,n,transforms", COMPILE_CASES)
+def test_generated_source_compiles(jit_cache, op, mode, sign, tw4, n, transforms):
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    assert L.lib().sipFftJitCompileCheck(op, mode, sign, tw4, n, transforms) == L.ACL_SUCCESS
+    files = list(jit_cache.glob("sk_*.cubin"))
+    assert files, "cubin not cached"
+    # a second request is served from the cache
+    assert L.lib().sipFftJitCompileCheck(op, mode, sign, tw4, n, transforms) == L.ACL_SUCCESS
+    assert sorted(jit_cache.glob("sk_*.cubin")) == sorted(files)
+
+
+def test_unsupported_configurations():
+    lib = L.lib()
+    assert lib.sipFftJitCompileCheck(OP_C2C, ROWS, -1, 0, 2656, 64) == L.ACL_ERROR_API_NOT_SUPPORT  # factor 83
+    assert lib.sipFftJitCompileCheck(OP_R2C_HALF, COLS, -1, 0, 1000, 64) == L.ACL_ERROR_API_NOT_SUPPORT
+    assert lib.sipFftJitCompileCheck(OP_C2C, ROWS, -1, 0, 32768, 64) == L.ACL_ERROR_API_NOT_SUPPORT  # > one tile
+
+
+def _input(op, n_sizes, batch, seed):
+    rng = np.random.default_rng(seed)
+    ishape, idt, _, _ = shapes(op, n_sizes, batch)
+    if op == O.C2R:
+        return np.fft.rfftn(rng.uniform(-1, 1, (batch, *n_sizes)), axes=tuple(range(1, len(n_sizes) + 1))
+                            ).astype(np.complex64).reshape(ishape)
+    if idt == np.float32:
+        return rng.uniform(-1, 1, ishape).astype(np.float32)
+    return (rng.standard_normal(ishape) + 1j * rng.standard_normal(ishape)).astype(np.complex64)
+
+
+def _gpu(torch, op, direction, sizes, batch, x, jit):
+    from sip_b200.fft import check
+
+    _, _, oshape, odt = shapes(op, sizes, batch)
+    xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    yt = torch.zeros(oshape, dtype=torch.complex64 if odt == np.complex64 else torch.float32, device="cuda")
+    h = _plan(op, direction, sizes, batch, jit)
+    used = any(s.get("jit") for s in h.describe()["steps"])
+    h.bind_workspace()
+    s = torch.cuda.Stream()
+    check(h.set_stream(s), "stream")
+    fn = {O.C2C: h.exec_c2c, O.R2C: h.exec_r2c, O.C2R: h.exec_c2r}[op]
+    settle()
+    check(fn(xt, yt), "exec")
+    check(h.synchronize(), "sync")
+    out = yt.cpu().numpy()
+    h.destroy()
+    return out, used
+
+
+# (op, direction, sizes, batch): rows of lengths without compiled kernels,
+# odd real lengths (pairs), 2-D column passes and four-step lengths.
+GPU_CASES = [
+    (O.C2C, O.FORWARD, [3840], 37), (O.C2C, O.INVERSE, [2016], 21), (O.C2C, O.FORWARD, [544], 50),
+    (O.C2C, O.INVERSE, [6720], 9), (O.C2C, O.FORWARD, [8160], 5), (O.C2C, O.INVERSE, [2944], 11),
+    (O.C2C, O.FORWARD, [16337], 3), (O.C2C, O.INVERSE, [5400], 7), (O.C2C, O.FORWARD, [96], 300),
+    (O.R2C, O.FORWARD, [6688], 13), (O.C2R, O.INVERSE, [6720], 13), (O.R2C, O.INVERSE, [5000], 9),
+    (O.R2C, O.FORWARD, [2001], 15), (O.C2R, O.INVERSE, [2001], 15), (O.C2R, O.FORWARD, [729], 40),
+    (O.C2C, O.FORWARD, [243, 300], 3), (O.C2C, O.INVERSE, [625, 96], 2),
+    (O.C2C, O.FORWARD, [3840 * 64], 2), (O.C2C, O.INVERSE, [243 * 625], 2),
+    (O.R2C, O.FORWARD, [2 * 3840 * 48], 2), (O.C2R, O.INVERSE, [2 * 3840 * 48], 2),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op,direction,sizes,batch", GPU_CASES)
+def test_jit_parity(cuda, jit_cache, op, direction, sizes, batch):
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    x = _input(op, sizes, batch, seed=sum(sizes) + batch)
+    out, used = _gpu(cuda, op, direction, sizes, batch, x, jit=1)
+    assert used, "no step was compiled at run time"
+    err = O.rel_l2(out, O.fp64(op, direction, x, sizes))
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+    gen, used_gen = _gpu(cuda, op, direction, sizes, batch, x, jit=2)
+    assert not used_gen
+    assert O.rel_l2(out, gen) <= 2 * REL_L2_TOL
