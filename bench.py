@@ -363,6 +363,11 @@ def published_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> d
             check(h.make_plan_1d(sizes[0], t, d, batch), "plan")
         else:
             check(h.make_plan_2d(sizes[0], sizes[1], t, d, batch), "plan")
+        # kernels of the plan's tile steps: compiled size-specialized ("sk"),
+        # compiled at run time by NVRTC on first use ("jit", outside the
+        # timing), or the generic runtime-radix kernel ("generic")
+        kinds = sorted({("jit" if st.get("jit") else "sk" if st.get("sk") else "generic")
+                        for st in h.describe()["steps"] if "sk" in st})
         h.bind_workspace(dev)
         check(h.set_stream(stream), "stream")
         torch.cuda.synchronize()
@@ -375,7 +380,8 @@ def published_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> d
         e1.record(stream)
         torch.cuda.synchronize()
         us = e0.elapsed_time(e1) / steps * 1e3
-        out[name] = {"us": round(us, 2), "reference_us_ascend950": ref_us, "ratio": round(ref_us / us, 2)}
+        out[name] = {"us": round(us, 2), "reference_us_ascend950": ref_us, "ratio": round(ref_us / us, 2),
+                     "kernels": kinds}
         h.destroy()
         del x, y
     return out

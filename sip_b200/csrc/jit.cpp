@@ -222,9 +222,10 @@ bool sk_jit_available() {
 }
 
 bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out) {
-    const bool row_op = op == OP_R2C_HALF || op == OP_C2R_HALF || op == OP_R2C_PAIR || op == OP_C2R_PAIR;
-    if (op != OP_C2C && !row_op) return false;
-    if (row_op && (mode != SK_ROWS || tw4)) return false;
+    const bool real_op = op == OP_R2C_HALF || op == OP_C2R_HALF || op == OP_R2C_PAIR || op == OP_C2R_PAIR;
+    if (op != OP_C2C && op != OP_PC && !real_op) return false;
+    if (real_op && (mode != SK_ROWS || tw4)) return false;
+    if (op == OP_PC && mode != SK_ROWS) return false;
     if ((op == OP_R2C_PAIR || op == OP_C2R_PAIR) && n % 2 == 0) return false;
     if (n < 8 || n > kMaxTileN) return false;
     JitCfg c;

@@ -188,7 +188,10 @@ int sk_mode_of(int op, int n, const AxisIO& io) {
         case OP_C2R_PAIR: in_row = n / 2 + 1; break;
         default: break;
     }
-    if (io.outer == 1 && io.in_stride == 1 && io.out_stride == 1 && io.in_idist == in_row && io.out_idist == out_row)
+    // rows: contiguous within a tile; successive outer indices continue the
+    // same row pitch (the tile decode keeps a tile inside one outer index)
+    if (io.in_stride == 1 && io.out_stride == 1 && io.in_idist == in_row && io.out_idist == out_row &&
+        (io.outer == 1 || (io.in_odist == io.inner * in_row && io.out_odist == io.inner * out_row)))
         return SK_ROWS;
     if (op != OP_C2C) return -1;
     if (io.in_idist == 1 && io.out_idist == 1) return SK_COLS;

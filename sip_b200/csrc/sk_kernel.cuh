@@ -106,10 +106,25 @@ struct SkCfg {
     // Minimum resident CTAs per SM (register-allocation target), chosen
     // per configuration so that the kernel does not spill.
     static constexpr int MINB = MINB_;
+    // Pass 0 reads the staged input (false) or the work layout (true: the
+    // inverse half of a pulse-compression tile, SkView below).
+    static constexpr bool WORK_IN = false;
 
     static_assert(span(NP) == N, "radices must multiply to N");
     static_assert(OP != OP_C2C || MODE != SK_COLS || true, "");
-    static_assert(!(TW4 && OP != OP_C2C), "cross twiddles are C2C only");
+    static_assert(!(TW4 && OP != OP_C2C && OP != OP_PC), "cross twiddles are C2C / pulse only");
+};
+
+// A configuration seen with another operation, direction and pass-0 source:
+// the two halves of an OP_PC tile run the same radix passes as
+// SkView<K, OP_PC, -1, false> (forward, staged input, last pass to shared
+// memory) and SkView<K, OP_C2C, +1, true> (inverse, from the work layout,
+// last pass to global memory with the C2C epilogue).
+template <class K, int OP_, int SIGN_, bool WORK_IN_>
+struct SkView : K {
+    static constexpr int OP = OP_;
+    static constexpr int SIGN = SIGN_;
+    static constexpr bool WORK_IN = WORK_IN_;
 };
 
 // Column index of slot q of a C2R_4A tile (-1 when the slot is unused).
@@ -297,7 +312,7 @@ SIP_HD float2 sk_c2r4a_input(const TileArgs& a, const TileCtx& c, const float2* 
 template <class K>
 SIP_HD float2 sk_input(const TileArgs& a, const TileCtx& c, const float2* stage, int q, int n) {
     constexpr int N = K::N;
-    if constexpr (K::OP == OP_C2C) {
+    if constexpr (K::OP == OP_C2C || K::OP == OP_PC) {
         const float2 v = K::MODE == SK_COLS ? stage[n * K::P + q] : stage[q * N + n];
         return maybe_conj(v, (a.flags & TF_CONJ_IN) != 0);
     } else if constexpr (K::OP == OP_R2C_HALF || K::OP == OP_R2C_4B) {
@@ -369,7 +384,7 @@ struct SkPass {
                 butterfly_index(b, q, j);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    if constexpr (PASS == 0)
+                    if constexpr (PASS == 0 && !K::WORK_IN)
                         rg.v[s][r] = sk_input<K>(a, c, buf, q, j + r * NR);
                     else
                         rg.v[s][r] = buf[q * K::LD + K::idx(j + r * NR)];
@@ -462,7 +477,7 @@ struct SkPass {
 
 template <class K>
 constexpr bool sk_last_to_smem() {
-    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR || K::OP == OP_R2C_4B;
+    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR || K::OP == OP_R2C_4B || K::OP == OP_PC;
 }
 
 // R2C value X[k] from Z[k] and Z[M-k] (formula of tile_io.cuh
@@ -581,6 +596,22 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
     }
 }
 
+// OP_PC: the spectra in the work layout times the filter spectrum, element
+// k of transform q times mul[(i0 + q) * mul_pitch_p + k * mul_pitch_k]
+// (conjugated under TF_MUL_CONJ), as tile_io.cuh mul_tile.
+template <class K>
+SIP_HD void sk_mul(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
+    const bool cj = (a.flags & TF_MUL_CONJ) != 0;
+    const int total = c.cnt * K::N;
+    for (int f = tid; f < total; f += K::T) {
+        const int q = f / K::N;
+        const int k = f - q * K::N;
+        const float2 m = SIP_LDG(a.mul + (long long)(c.i0 + q) * a.mul_pitch_p + (long long)k * a.mul_pitch_k);
+        float2& v = buf[q * K::LD + K::idx(k)];
+        v = c_mul(v, maybe_conj(m, cj));
+    }
+}
+
 }  // namespace sipfft
 
 // ------------------------------------------------------------ kernel
@@ -640,6 +671,15 @@ __global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a)
         if constexpr (K::OP == OP_R2C_PAIR || K::OP == OP_C2R_PAIR) {
             sk_zero_missing<K>(tid, a, c, cur);
             __syncthreads();
+        }
+        if constexpr (K::OP == OP_PC) {
+            // forward FFT, filter, inverse FFT, all in shared memory
+            sk_run<SkView<K, OP_PC, -1, false>, 0>(tid, a, c, cur);
+            sk_mul<K>(tid, a, c, cur);
+            __syncthreads();
+            sk_run<SkView<K, OP_C2C, 1, true>, 0>(tid, a, c, cur);
+            __syncthreads();
+            continue;
         }
         sk_run<K, 0>(tid, a, c, cur);
         if constexpr (sk_last_to_smem<K>()) sk_post<K>(tid, a, c, cur);

@@ -126,6 +126,12 @@ void emu_sk_run(const TileArgs& a) {
         for (auto& v : buf) v = make_float2(nan, nan);
         for (int tid = 0; tid < K::T; ++tid) sk_stage<K>(tid, a, c, buf.data());
         for (int tid = 0; tid < K::T; ++tid) sk_zero_missing<K>(tid, a, c, buf.data());
+        if constexpr (K::OP == OP_PC) {
+            emu_sk_passes<SkView<K, OP_PC, -1, false>, 0>(a, c, buf.data());
+            for (int tid = 0; tid < K::T; ++tid) sk_mul<K>(tid, a, c, buf.data());
+            emu_sk_passes<SkView<K, OP_C2C, 1, true>, 0>(a, c, buf.data());
+            continue;
+        }
         emu_sk_passes<K, 0>(a, c, buf.data());
         if constexpr (sk_last_to_smem<K>())
             for (int tid = 0; tid < K::T; ++tid) sk_post<K>(tid, a, c, buf.data());
@@ -162,6 +168,14 @@ const std::vector<SkEntry>& sk_registry() {
 #define SIP_EMU_SK(S, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, ...) \
     v.push_back(emu_entry<SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, TWB, __VA_ARGS__>, STAGES>({__VA_ARGS__}));
         SIP_SK_CONFIGS(SIP_EMU_SK)
+        // Pulse-compression tiles (the library compiles these at run time,
+        // csrc/jit.cpp): rows of 1000, Bluestein's 2025 for n = 1009, and the
+        // four-step pass P (cross twiddles) of 2^18 = 512 x 512 and of
+        // Bluestein's 40500 = 180 x 225 for n = 20011.
+        SIP_EMU_SK(0, 1000, 4, 128, OP_PC, SK_ROWS, 1, false, 2, 4, 1, 10, 10, 10)
+        SIP_EMU_SK(0, 2025, 2, 192, OP_PC, SK_ROWS, 1, false, 2, 2, 1, 15, 15, 9)
+        SIP_EMU_SK(0, 512, 8, 256, OP_PC, SK_ROWS, 1, true, 2, 2, 1, 32, 16)
+        SIP_EMU_SK(0, 225, 16, 256, OP_PC, SK_ROWS, 1, true, 2, 2, 1, 15, 15)
 #undef SIP_EMU_SK
         return v;
     }();

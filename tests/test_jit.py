@@ -18,7 +18,7 @@ from tests.fftcase import settle, shapes
 
 REL_L2_TOL = 1e-6
 
-OP_C2C, OP_R2C_HALF, OP_C2R_HALF, OP_R2C_PAIR, OP_C2R_PAIR = 0, 1, 2, 3, 4
+OP_C2C, OP_R2C_HALF, OP_C2R_HALF, OP_R2C_PAIR, OP_C2R_PAIR, OP_PC = 0, 1, 2, 3, 4, 7
 ROWS, COLS, ROWS_T = 0, 1, 2
 
 
@@ -84,6 +84,8 @@ COMPILE_CASES = [
     (OP_C2R_HALF, ROWS, 1, 0, 3344, 8192),
     (OP_R2C_PAIR, ROWS, -1, 0, 2001, 1000),
     (OP_C2R_PAIR, ROWS, 1, 0, 2001, 1000),
+    (OP_PC, ROWS, 1, 0, 10800, 8192),       # pulse compression tile (Bluestein's convolution)
+    (OP_PC, ROWS, 1, 1, 225, 9000),         # four-step pulse pass P
 ]
 
 
@@ -164,3 +166,49 @@ def test_jit_parity(cuda, jit_cache, op, direction, sizes, batch):
     gen, used_gen = _gpu(cuda, op, direction, sizes, batch, x, jit=2)
     assert not used_gen
     assert O.rel_l2(out, gen) <= 2 * REL_L2_TOL
+
+
+# Pulse compression (OP_PC tiles: forward FFT, filter, inverse FFT in shared
+# memory) compiled at run time: one-tile rows and the four-step pass P.
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,batch", [(1000, 33), (10800, 3), (3840 * 64, 2)])
+@pytest.mark.parametrize("flags", [1, 3])
+def test_jit_pulse(cuda, jit_cache, n, batch, flags):
+    from sip_b200.fft import FftHandle, check
+    from tests.test_emu_pulse import signal
+
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    torch = cuda
+    x = signal(n, batch, 20261203 + n)
+    filt = O.chirp_spectrum(n)
+    xt = torch.from_numpy(x).cuda()
+    ft = torch.from_numpy(filt.astype(np.complex64)).cuda()
+    yt = torch.zeros_like(xt)
+    h = FftHandle()
+    check(h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, 1), "hint")
+    check(h.make_plan_pulse_1d(n, batch, ft.data_ptr(), flags), "sipFftMakePlanPulse1D")
+    assert any(s.get("jit") and s.get("op") == 7 for s in h.describe()["steps"])
+    h.bind_workspace()
+    s = torch.cuda.Stream()
+    check(h.set_stream(s), "stream")
+    settle()
+    check(h.exec_c2c(xt, yt), "exec")
+    s.synchronize()
+    want = O.pulse(x, filt, conj=bool(flags & 1), scale=bool(flags & 2))
+    assert O.rel_l2(yt.cpu().numpy(), want) <= REL_L2_TOL
+    h.destroy()
+
+
+# Bluestein lengths: the convolution runs as a run-time compiled OP_PC tile.
+@pytest.mark.gpu
+@pytest.mark.parametrize("op,direction,n,batch", [(O.R2C, O.FORWARD, 5312, 6), (O.C2R, O.INVERSE, 5344, 6),
+                                                  (O.C2C, O.INVERSE, 6752, 5), (O.C2C, O.FORWARD, 20011, 2)])
+def test_jit_bluestein(cuda, jit_cache, op, direction, n, batch):
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    x = _input(op, [n], batch, seed=n)
+    out, used = _gpu(cuda, op, direction, [n], batch, x, jit=1)
+    assert used
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
