@@ -584,12 +584,10 @@ AspbStatus sipFftTakeDeviceErrors(unsigned* errors) {
 
 AspbStatus sipFftJitCompileCheck(int op, int mode, int sign, int tw4, int n, long long transforms) {
     sipfft::JitCfg c;
-    if (!sipfft::sk_jit_available() ||
-        !sipfft::sk_jit_choose(op, mode, sign, tw4 != 0, n, transforms, &c))
+    if (!sipfft::sk_jit_available() || !sipfft::sk_jit_choose(op, mode, sign, tw4 != 0, n, transforms, &c))
         return ACL_ERROR_API_NOT_SUPPORT;
-    std::vector<char> cubin;
-    std::string lowered, err;
-    if (!sipfft::sk_jit_compile(c, &cubin, &lowered, &err)) {
+    std::string err;
+    if (!sipfft::sk_jit_select(op, mode, sign, tw4 != 0, n, transforms, &c, &err)) {
         std::fprintf(stderr, "sipFftJitCompileCheck: %s\n", err.c_str());
         return ACL_ERROR_INTERNAL_ERROR;
     }

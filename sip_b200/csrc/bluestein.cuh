@@ -6,10 +6,12 @@
 //   a_j = x_j c_j (j < n), 0 (n <= j < m)
 //   y   = IFFT_m(FFT_m(a) . FFT_m(b)) / m,   b_j = conj(c_j), b_{m-j} = b_j
 //   X_k = c_k y_k                              (k < n)
-// since exp(s 2 pi i j k / n) = c_j c_k conj(c_{k-j}).  R2C and C2R run the
-// complex transform: the pre pass promotes real input, or expands a half
-// spectrum to its Hermitian full length; the post pass keeps n/2 + 1 bins,
-// or the real part.  (Reference: the large-prime routes of
+// since exp(s 2 pi i j k / n) = c_j c_k conj(c_{k-j}).  Odd-length R2C and
+// C2R run the complex transform: the pre pass promotes real input, or
+// expands a half spectrum to its Hermitian full length; the post pass keeps
+// n/2 + 1 bins, or the real part.  Even real lengths run the half-length
+// complex transform through Bluestein instead (the planner's real pre /
+// post passes around a BLUE_C2C of n/2).  (Reference: the large-prime routes of
 // core/fft/fft_api.cpp:84-132 send such lengths to a cube-tail / DFT core.)
 #pragma once
 
@@ -28,6 +30,7 @@ struct BluesteinArgs {
     long long in_pitch;   // input row pitch (float2 units; floats for R2C input)
     long long out_pitch;  // output row pitch (float2 units; floats for C2R output)
     int kind;             // BlueKind
+    float scale = 1.0f;   // factor on the post pass's outputs
 };
 
 // Pre pass value a_j of row `row` (j < m).
@@ -56,7 +59,8 @@ SIP_HD float2 blue_pre_elem(const BluesteinArgs& a, long long row, long long j) 
 // Post pass: output k of row `row` from the convolution row y (m values).
 SIP_HD void blue_post_elem(const BluesteinArgs& a, long long row, long long k) {
     const float2* y = static_cast<const float2*>(a.src) + row * a.m;
-    const float2 v = c_mul(SIP_LDG(y + k), SIP_LDG(a.chirp + k));
+    float2 v = c_mul(SIP_LDG(y + k), SIP_LDG(a.chirp + k));
+    if (a.scale != 1.0f) v = c_scale(v, a.scale);
     if (a.kind == BLUE_C2R)
         static_cast<float*>(a.dst)[row * a.out_pitch + k] = v.x;
     else

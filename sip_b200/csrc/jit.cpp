@@ -7,6 +7,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -16,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <thread>
 
 #include "plan.h"
 #include "sk_kernel.cuh"
@@ -142,6 +144,12 @@ std::mutex g_jit_mu;
 std::deque<SkEntry> g_jit_entries;  // stable addresses
 std::map<std::string, SkEntry*> g_jit_index;
 std::map<std::string, const void*> g_jit_kernels;  // name expression -> loaded kernel
+struct JitBinary {
+    std::vector<char> cubin;
+    std::string lowered;
+    int spill = 0;
+};
+std::map<std::string, JitBinary> g_jit_cubins;  // name expression -> compiled in this process
 
 JitCfg cfg_of(const SkEntry& e) {
     JitCfg c;
@@ -187,23 +195,25 @@ std::string cache_dir() {
     return d;
 }
 
-// Cache file: "SIPJIT1\n<lowered name>\n<cubin bytes>".
-bool cache_read(const std::string& path, std::vector<char>* cubin, std::string* lowered) {
+// Cache file: "SIPJIT2\n<lowered name>\n<spill bytes>\n<cubin bytes>".
+bool cache_read(const std::string& path, std::vector<char>* cubin, std::string* lowered, int* spill) {
     std::ifstream f(path, std::ios::binary);
     if (!f) return false;
-    std::string magic;
-    if (!std::getline(f, magic) || magic != "SIPJIT1") return false;
+    std::string magic, sp;
+    if (!std::getline(f, magic) || magic != "SIPJIT2") return false;
     if (!std::getline(f, *lowered) || lowered->empty()) return false;
+    if (!std::getline(f, sp) || sp.empty()) return false;
+    *spill = std::atoi(sp.c_str());
     cubin->assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
     return !cubin->empty();
 }
 
-void cache_write(const std::string& path, const std::vector<char>& cubin, const std::string& lowered) {
+void cache_write(const std::string& path, const std::vector<char>& cubin, const std::string& lowered, int spill) {
     const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
     {
         std::ofstream f(tmp, std::ios::binary);
         if (!f) return;
-        f << "SIPJIT1\n" << lowered << "\n";
+        f << "SIPJIT2\n" << lowered << "\n" << spill << "\n";
         f.write(cubin.data(), (std::streamsize)cubin.size());
         if (!f) {
             std::remove(tmp.c_str());
@@ -221,7 +231,7 @@ bool sk_jit_available() {
     return nvrtc().ok;
 }
 
-bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out) {
+bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out, int values) {
     const bool real_op = op == OP_R2C_HALF || op == OP_C2R_HALF || op == OP_R2C_PAIR || op == OP_C2R_PAIR;
     if (op != OP_C2C && op != OP_PC && !real_op) return false;
     if (real_op && (mode != SK_ROWS || tw4)) return false;
@@ -241,7 +251,7 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     // runs of 16 adjacent transforms (128-byte segments) for the column
     // modes; at most SIP_FFT_JIT_E (32) values per thread and pass
     const int tile_values = std::max(64, env_int("SIP_FFT_JIT_TILE", 4096));
-    const int per_thread = std::max(8, env_int("SIP_FFT_JIT_E", 32));
+    const int per_thread = std::max(8, values > 0 ? values : env_int("SIP_FFT_JIT_E", 32));
     long long P = mode == SK_ROWS ? std::max(1, tile_values / n) : 16;
     P = std::min<long long>(P, transforms);
     int T = 0;
@@ -278,7 +288,19 @@ std::string sk_jit_name_expr(const JitCfg& c) {
     return s.str();
 }
 
-bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err) {
+// Spill stores the compiler's resource report (--ptxas-options=-v) states.
+int spill_bytes(const std::string& log) {
+    int total = 0;
+    const std::string key = " bytes spill stores";
+    for (size_t pos = log.find(key); pos != std::string::npos; pos = log.find(key, pos + 1)) {
+        size_t b = pos;
+        while (b > 0 && std::isdigit((unsigned char)log[b - 1])) --b;
+        if (b < pos) total += std::atoi(log.substr(b, pos - b).c_str());
+    }
+    return total;
+}
+
+bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err, int* spill) {
     const Nvrtc& api = nvrtc();
     if (!api.ok) {
         *err = "NVRTC is not available";
@@ -300,7 +322,21 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     std::snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
     const std::string dir = cache_dir();
     const std::string path = dir.empty() ? "" : dir + "/sk_" + hex + ".cubin";
-    if (!path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(path, cubin, lowered)) return true;
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        auto it = g_jit_cubins.find(expr);
+        if (it != g_jit_cubins.end()) {
+            *cubin = it->second.cubin;
+            *lowered = it->second.lowered;
+            *spill = it->second.spill;
+            return true;
+        }
+    }
+    if (!path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(path, cubin, lowered, spill)) {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        g_jit_cubins[expr] = {*cubin, *lowered, *spill};
+        return true;
+    }
 
     nvrtcProgram prog = nullptr;
     if (api.create(&prog, src.c_str(), "sip_fft_jit.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
@@ -308,11 +344,11 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
         *err = "nvrtcCreateProgram failed";
         return false;
     }
-    // SIP_FFT_JIT_VERBOSE=1 prints the compiler's resource report (registers,
-    // spills) of every kernel compiled here
+    // the compiler's resource report (registers, spills) steers the choice
+    // between configurations; SIP_FFT_JIT_VERBOSE=1 prints it
     const bool verbose = env_int("SIP_FFT_JIT_VERBOSE", 0) != 0;
     std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
-    if (verbose) opts.push_back("--ptxas-options=-v");
+    opts.push_back("--ptxas-options=-v");
     bool ok = api.add_name(prog, expr.c_str()) == NVRTC_SUCCESS;
     const nvrtcResult rc = ok ? api.compile(prog, (int)opts.size(), opts.data()) : NVRTC_ERROR_INVALID_INPUT;
     size_t ls = 0;
@@ -341,14 +377,71 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
         *err = "NVRTC produced no kernel for " + expr;
         return false;
     }
-    if (!path.empty()) cache_write(path, *cubin, *lowered);
+    *spill = spill_bytes(log);
+    if (!path.empty()) cache_write(path, *cubin, *lowered, *spill);
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    g_jit_cubins[expr] = {*cubin, *lowered, *spill};
+    return true;
+}
+
+bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out,
+                   std::string* err) {
+    // Candidates: at most 32 values per thread and pass (the default), then
+    // 16 and 48, compiled concurrently; the first in that order without
+    // register spills wins, else the one with the fewest spilled bytes.
+    // SIP_FFT_JIT_E pins one.
+    std::vector<int> tries = {32, 16, 48};
+    if (env_int("SIP_FFT_JIT_E", 0) > 0) tries = {env_int("SIP_FFT_JIT_E", 0)};
+    std::vector<JitCfg> cands;
+    std::vector<std::string> seen;
+    for (int v : tries) {
+        JitCfg c;
+        if (!sk_jit_choose(op, mode, sign, tw4, n, transforms, &c, v)) continue;
+        const std::string expr = sk_jit_name_expr(c);
+        if (std::find(seen.begin(), seen.end(), expr) != seen.end()) continue;
+        seen.push_back(expr);
+        cands.push_back(c);
+    }
+    if (cands.empty()) {
+        *err = "no run-time configuration for this step";
+        return false;
+    }
+    struct Result {
+        bool ok = false;
+        int spill = 0;
+        std::string err;
+    };
+    std::vector<Result> res(cands.size());
+    std::vector<std::thread> workers;
+    for (size_t i = 0; i < cands.size(); ++i)
+        workers.emplace_back([&, i] {
+            std::vector<char> cubin;
+            std::string lowered;
+            res[i].ok = sk_jit_compile(cands[i], &cubin, &lowered, &res[i].err, &res[i].spill);
+        });
+    for (auto& w : workers) w.join();
+    int best = -1;
+    for (size_t i = 0; i < cands.size(); ++i) {
+        if (!res[i].ok) {
+            *err = res[i].err;
+            continue;
+        }
+        if (best < 0 || res[i].spill < res[best].spill) best = (int)i;
+        if (res[i].spill == 0) break;
+    }
+    if (best < 0) return false;
+    *out = cands[best];
     return true;
 }
 
 const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms) {
     if (!sk_jit_available()) return nullptr;
     JitCfg c;
-    if (!sk_jit_choose(op, mode, sign, tw4, n, transforms, &c)) return nullptr;
+    std::string err;
+    if (!sk_jit_select(op, mode, sign, tw4, n, transforms, &c, &err)) {
+        if (env_int("SIP_FFT_JIT_VERBOSE", 0) != 0) std::fprintf(stderr, "sip_fft jit: %s\n", err.c_str());
+        return nullptr;  // the generic tile kernel runs the step
+    }
     const std::string key = sk_jit_name_expr(c);
     std::lock_guard<std::mutex> lk(g_jit_mu);
     auto it = g_jit_index.find(key);
@@ -386,7 +479,8 @@ const void* sk_jit_load(const SkEntry* entry) {
     }
     std::vector<char> cubin;
     std::string lowered, err;
-    if (!sk_jit_compile(c, &cubin, &lowered, &err)) throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, err);
+    int spill = 0;
+    if (!sk_jit_compile(c, &cubin, &lowered, &err, &spill)) throw PlanError(AsdSip::ACL_ERROR_INTERNAL_ERROR, err);
     cudaLibrary_t lib = nullptr;
     cudaError_t e = cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e != cudaSuccess)

@@ -7,11 +7,13 @@
 // stages, register target) and have NVRTC compile sk_fft_kernel<that
 // configuration> from the library's own kernel headers, embedded in the
 // library at build time.  Compilation happens once per configuration and
-// process, when a plan that uses it is first prepared on a device, and the
-// cubin is kept in an on-disk cache (SIP_FFT_JIT_CACHE, default
+// process, and the cubin is kept in an on-disk cache (SIP_FFT_JIT_CACHE, default
 // $HOME/.cache/sip_fft_jit) keyed by a hash of the source, the headers, the
-// options and the NVRTC version.  NVRTC is loaded with dlopen; without it
-// no run-time entry is offered and the generic kernel runs.
+// options and the NVRTC version.  The configuration is chosen and compiled
+// when the plan is made (CPU work; the compiler's register report rejects
+// configurations that spill) and loaded when the plan is first prepared on
+// a device.  NVRTC is loaded with dlopen; without it no run-time entry is
+// offered and the generic kernel runs.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,16 +33,25 @@ struct JitCfg {
     int LD = 0, smem = 0;
 };
 
-// Host-side choice of a configuration (no CUDA or NVRTC calls).
-bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out);
+// Host-side configuration for at most `values` values per thread and pass
+// (0: SIP_FFT_JIT_E or 32); no CUDA or NVRTC calls.
+bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out, int values = 0);
+
+// The configuration the planner uses: candidates of sk_jit_choose compiled
+// in turn (32, 16, 48 values per thread) until one has no register spills
+// (else the fewest spilled bytes).  Compiles on the CPU; false with a
+// message when nothing compiles.
+bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out,
+                   std::string* err);
 
 // The NVRTC source and the kernel's name expression for a configuration.
 std::string sk_jit_source();
 std::string sk_jit_name_expr(const JitCfg& c);
 
-// Compiles a configuration to a cubin (through the disk cache); returns
-// false with the compiler log in *err on failure.
-bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err);
+// Compiles a configuration to a cubin (through the process and disk
+// caches) with its spilled bytes; returns false with the compiler log in
+// *err on failure.
+bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err, int* spill);
 
 // Compiles and loads the kernel of a run-time entry (from sk_jit_entry)
 // and stores it in the entry; returns the kernel.  Throws PlanError when

@@ -593,13 +593,21 @@ constexpr long long kMaxBluesteinN = 1LL << 22;
 
 // Bluestein's algorithm (bluestein.cuh): pre pass into the workspace, the
 // fused pulse chain of length m in place there (filter = the plan's
-// Bluestein table, scale 1/m), post pass into the output.  Workspace:
-// [0, conv) the convolution rows, then the four-step intermediate of m.
-void add_bluestein(FftPlan& plan, int kind, long long n, long long batch) {
+// Bluestein table, scale 1/m), post pass into the destination.  Workspace
+// from ws_off: the convolution rows, then the four-step intermediate of m.
+struct BlueIO {
+    Loc src = Loc::In, dst = Loc::Out;
+    size_t src_off = 0, dst_off = 0;
+    size_t ws_off = 0;   // start of the Bluestein's own workspace
+    int sign = 0;        // 0: the plan's direction
+    float scale = 1.0f;  // on the post pass's outputs
+};
+
+void add_bluestein(FftPlan& plan, int kind, long long n, long long batch, const BlueIO& io = BlueIO{}) {
     if (n > kMaxBluesteinN)
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " needs Bluestein above 2^22");
     const long long m = bluestein_length(n);
-    const int sign = plan.forward() ? -1 : 1;
+    const int sign = io.sign != 0 ? io.sign : (plan.forward() ? -1 : 1);
     const size_t conv = ((size_t)(batch * m * 8) + 255) / 256 * 256;
     Step pre;
     pre.kind = StepKind::Blue;
@@ -612,14 +620,17 @@ void add_bluestein(FftPlan& plan, int kind, long long n, long long batch) {
     pre.blue_n = n;
     pre.blue_m = m;
     pre.blue_sign = sign;
-    pre.src = Loc::In;
+    pre.src = io.src;
+    pre.src_off = io.src_off;
     pre.dst = Loc::Ws;
+    pre.dst_off = io.ws_off;
     pre.what = "bluestein pre n=" + std::to_string(n) + " m=" + std::to_string(m);
     plan.steps.push_back(pre);
     const size_t first = plan.steps.size();
     PulseIO pio;
     pio.src = pio.dst = Loc::Ws;
-    pio.scratch_off = conv;
+    pio.src_off = pio.dst_off = io.ws_off;
+    pio.scratch_off = io.ws_off + conv;
     pio.mul_table = 1;
     add_pulse_steps(plan, m, batch, nullptr, kPulseScale, pio);
     for (size_t i = first; i < plan.steps.size(); ++i) {
@@ -631,11 +642,67 @@ void add_bluestein(FftPlan& plan, int kind, long long n, long long batch) {
     post.blue_post = true;
     post.blue.in_pitch = m;
     post.blue.out_pitch = kind == BLUE_R2C ? n / 2 + 1 : n;
+    post.blue.scale = io.scale;
     post.src = Loc::Ws;
-    post.dst = Loc::Out;
+    post.src_off = io.ws_off;
+    post.dst = io.dst;
+    post.dst_off = io.dst_off;
     post.what = "bluestein post n=" + std::to_string(n);
     plan.steps.push_back(post);
-    plan.workspace_need = std::max(plan.workspace_need, conv + (m > kMaxTileN ? (size_t)(batch * m * 8) : 0));
+    plan.workspace_need =
+        std::max(plan.workspace_need, io.ws_off + conv + (m > kMaxTileN ? (size_t)(batch * m * 8) : 0));
+}
+
+// Even real length n whose half length m = n/2 needs Bluestein: the
+// half-length complex transform (real rows read as m complex values) runs
+// through Bluestein, with the real post-process (R2C) after it or the real
+// pre-process (C2R) before it, as the large-real path does around a
+// four-step C2C.  The convolution is half as long as the full-length
+// complex Bluestein's.  Workspace: [0, z) the m-point rows, then the
+// Bluestein's own.
+void add_real_bluestein_half(FftPlan& plan, bool r2c, long long n, long long rows) {
+    const long long m = n / 2;
+    const size_t zbytes = (size_t)(rows * m * 8);
+    const size_t zoff = (zbytes + 255) / 256 * 256;
+    Step pp;
+    pp.kind = r2c ? StepKind::RealPost : StepKind::RealPre;
+    pp.real.m = m;
+    pp.real.rows = rows;
+    pp.real.conj = r2c ? (plan.forward() ? 0 : 1) : (plan.forward() ? 1 : 0);
+    pp.tw2_kind = 1;
+    pp.tw2_n = n;
+    pp.tw2_count = m + 1;
+    BlueIO io;
+    io.ws_off = zoff;
+    if (r2c) {
+        io.sign = -1;
+        io.src = Loc::In;
+        io.dst = Loc::Ws;
+        io.dst_off = 0;
+        add_bluestein(plan, BLUE_C2C, m, rows, io);
+        pp.real.in_pitch = m;
+        pp.real.out_pitch = m + 1;
+        pp.src = Loc::Ws;
+        pp.src_off = 0;
+        pp.dst = Loc::Out;
+        pp.what = "r2c post n=" + std::to_string(n);
+        plan.steps.push_back(pp);
+    } else {
+        pp.real.in_pitch = m + 1;
+        pp.real.out_pitch = m;
+        pp.src = Loc::In;
+        pp.dst = Loc::Ws;
+        pp.dst_off = 0;
+        pp.what = "c2r pre n=" + std::to_string(n);
+        plan.steps.push_back(pp);
+        io.sign = 1;
+        io.src = Loc::Ws;
+        io.src_off = 0;
+        io.dst = Loc::Out;
+        io.scale = 2.0f;
+        add_bluestein(plan, BLUE_C2C, m, rows, io);
+    }
+    plan.workspace_need = std::max(plan.workspace_need, zoff);
 }
 
 // Real transform along contiguous rows of length n (rows rows), one tile.
@@ -910,7 +977,10 @@ void build_steps(FftPlan& plan) {
             return;
         }
         if (!c2c && !real_direct(n)) {
-            add_bluestein(plan, r2c ? BLUE_R2C : BLUE_C2R, n, b);
+            if (n % 2 == 0 && n / 2 <= kMaxBluesteinN)
+                add_real_bluestein_half(plan, r2c, n, b);
+            else
+                add_bluestein(plan, r2c ? BLUE_R2C : BLUE_C2R, n, b);
             return;
         }
         if (c2c) {

@@ -51,6 +51,11 @@ def test_pulse_matches_fp64(emu, n, batch, flags):
     assert O.rel_l2(out, want) <= REL_L2_TOL, desc
     kinds = [s["what"].split(" n=")[0] for s in __import__("json").loads(desc)["steps"]]
     assert kinds == (["pulse rows"] if n <= 16384 else ["four-step A", "pulse rows", "pulse inverse columns"])
+    # the harness's size-specialized pulse tiles (rows of 1000; pass P of
+    # 2^18 = 512 x 512 with cross twiddles) run where they apply
+    pulse = [s for s in __import__("json").loads(desc)["steps"] if s["what"].startswith("pulse rows")]
+    if n in (1000, 1 << 18):
+        assert pulse[0]["sk"], desc
 
 
 def test_matched_filter_peaks_at_delay(emu):

@@ -94,11 +94,25 @@ def test_generated_source_compiles(jit_cache, op, mode, sign, tw4, n, transforms
     if not _nvrtc_present():
         pytest.skip("NVRTC not available")
     assert L.lib().sipFftJitCompileCheck(op, mode, sign, tw4, n, transforms) == L.ACL_SUCCESS
-    files = list(jit_cache.glob("sk_*.cubin"))
-    assert files, "cubin not cached"
-    # a second request is served from the cache
-    assert L.lib().sipFftJitCompileCheck(op, mode, sign, tw4, n, transforms) == L.ACL_SUCCESS
-    assert sorted(jit_cache.glob("sk_*.cubin")) == sorted(files)
+
+
+def test_disk_cache(tmp_path):
+    """A fresh process compiles into the cache directory; a second process
+    finds every cubin there and compiles nothing new."""
+    import subprocess
+    import sys
+
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    cache = tmp_path / "jit"
+    code = ("import sys; sys.path.insert(0, %r); from sip_b200 import _lib as L; "
+            "sys.exit(L.lib().sipFftJitCompileCheck(0, 0, -1, 0, 3840, 8192))" % os.getcwd())
+    env = dict(os.environ, SIP_FFT_JIT_CACHE=str(cache))
+    assert subprocess.run([sys.executable, "-c", code], env=env).returncode == 0
+    first = {p.name: p.stat().st_mtime_ns for p in cache.glob("sk_*.cubin")}
+    assert first, "cubin not cached"
+    assert subprocess.run([sys.executable, "-c", code], env=env).returncode == 0
+    assert {p.name: p.stat().st_mtime_ns for p in cache.glob("sk_*.cubin")} == first
 
 
 def test_unsupported_configurations():
