@@ -169,6 +169,7 @@ void prepare_device(FftPlan& plan) {
         }
         if (st.tw2_kind == 1) st.tw2 = root_table(device, st.tw2_n, st.tw2_count);
         if (st.tw2_kind == 2) st.tw2 = split_table(device, st.tw2_n, st.L.args.tw4_shift);
+        if (st.tw2_kind == 3) st.tw2 = chirp_table(device, st.blue_n, st.blue_sign);
         if (st.kind == StepKind::RealPost || st.kind == StepKind::RealPre) {
             st.real.tw = static_cast<const float2*>(st.tw2->ptr);
             continue;

@@ -149,7 +149,7 @@ struct JitBinary {
     std::string lowered;
     int spill = 0;
 };
-std::map<std::string, JitBinary> g_jit_cubins;  // name expression -> compiled in this process
+std::map<std::string, JitBinary> g_jit_cubins;  // cache key -> compiled in this process
 
 JitCfg cfg_of(const SkEntry& e) {
     JitCfg c;
@@ -308,10 +308,14 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     }
     const std::string src = sk_jit_source();
     const std::string expr = sk_jit_name_expr(c);
+    // SIP_FFT_JIT_PC_SPLIT=1: pulse tiles with out-of-line halves (sk_kernel.cuh)
+    std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
+    opts.push_back("--ptxas-options=-v");
+    if (env_int("SIP_FFT_JIT_PC_SPLIT", 0) != 0) opts.push_back("-DSIP_SK_PC_SPLIT=1");
     uint64_t h = 1469598103934665603ull;
     const int ver[2] = {api.major, api.minor};
     h = fnv1a(h, ver, sizeof(ver));
-    for (const char* o : kOptions) h = fnv1a(h, o, std::strlen(o) + 1);
+    for (const char* o : opts) h = fnv1a(h, o, std::strlen(o) + 1);
     h = fnv1a(h, src.data(), src.size());
     h = fnv1a(h, expr.data(), expr.size());
     for (int i = 0; i < kJitHeaderCount; ++i) {
@@ -324,7 +328,7 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     const std::string path = dir.empty() ? "" : dir + "/sk_" + hex + ".cubin";
     {
         std::lock_guard<std::mutex> lk(g_jit_mu);
-        auto it = g_jit_cubins.find(expr);
+        auto it = g_jit_cubins.find(hex);
         if (it != g_jit_cubins.end()) {
             *cubin = it->second.cubin;
             *lowered = it->second.lowered;
@@ -334,7 +338,7 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     }
     if (!path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(path, cubin, lowered, spill)) {
         std::lock_guard<std::mutex> lk(g_jit_mu);
-        g_jit_cubins[expr] = {*cubin, *lowered, *spill};
+        g_jit_cubins[hex] = {*cubin, *lowered, *spill};
         return true;
     }
 
@@ -347,8 +351,6 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     // the compiler's resource report (registers, spills) steers the choice
     // between configurations; SIP_FFT_JIT_VERBOSE=1 prints it
     const bool verbose = env_int("SIP_FFT_JIT_VERBOSE", 0) != 0;
-    std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
-    opts.push_back("--ptxas-options=-v");
     bool ok = api.add_name(prog, expr.c_str()) == NVRTC_SUCCESS;
     const nvrtcResult rc = ok ? api.compile(prog, (int)opts.size(), opts.data()) : NVRTC_ERROR_INVALID_INPUT;
     size_t ls = 0;
@@ -380,7 +382,7 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     *spill = spill_bytes(log);
     if (!path.empty()) cache_write(path, *cubin, *lowered, *spill);
     std::lock_guard<std::mutex> lk(g_jit_mu);
-    g_jit_cubins[expr] = {*cubin, *lowered, *spill};
+    g_jit_cubins[hex] = {*cubin, *lowered, *spill};
     return true;
 }
 
@@ -394,13 +396,32 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
     if (env_int("SIP_FFT_JIT_E", 0) > 0) tries = {env_int("SIP_FFT_JIT_E", 0)};
     std::vector<JitCfg> cands;
     std::vector<std::string> seen;
+    auto add = [&](const JitCfg& c) {
+        const std::string expr = sk_jit_name_expr(c);
+        if (std::find(seen.begin(), seen.end(), expr) != seen.end()) return;
+        seen.push_back(expr);
+        cands.push_back(c);
+    };
     for (int v : tries) {
         JitCfg c;
         if (!sk_jit_choose(op, mode, sign, tw4, n, transforms, &c, v)) continue;
-        const std::string expr = sk_jit_name_expr(c);
-        if (std::find(seen.begin(), seen.end(), expr) != seen.end()) continue;
-        seen.push_back(expr);
-        cands.push_back(c);
+        add(c);
+        // The register file is split over the SM's four schedulers: with one
+        // CTA per SM a block of 9-12 warps gets at most 168 registers per
+        // thread, one of 8 warps 255.  So each candidate is also tried with
+        // its threads rounded down to a multiple of 128 (more values per
+        // thread) and the register target left to the compiler.
+        if (c.T % 128 != 0 && c.T > 128) {
+            JitCfg r = c;
+            r.T = c.T / 128 * 128;
+            bool ok = true;
+            for (int rad : r.radices) {
+                const long long b = (long long)r.P * (n / rad);
+                if ((b + r.T - 1) / r.T * rad > 96) ok = false;  // values per thread and pass
+            }
+            r.minb = 1;
+            if (ok) add(r);
+        }
     }
     if (cands.empty()) {
         *err = "no run-time configuration for this step";

@@ -179,8 +179,9 @@ struct AxisIO {
 // One tile launch.  n = FFT length of each tile transform; rowlen = values
 // a shared-memory row must hold; transforms = inner * outer.
 // Layout mode of a step for the size-specialized kernels, or -1.
-int sk_mode_of(int op, int n, const AxisIO& io) {
+int sk_mode_of(int op, int n, const AxisIO& io, int blue_n = 0) {
     long long in_row = n, out_row = n;
+    if (blue_n > 0) in_row = out_row = blue_n;  // fused Bluestein rows (TF_BLUE)
     switch (op) {
         case OP_R2C_HALF: out_row = n + 1; break;
         case OP_C2R_HALF: in_row = n + 1; break;
@@ -204,7 +205,7 @@ int sk_mode_of(int op, int n, const AxisIO& io) {
 void try_specialize(Step& st, const AxisIO& io) {
     TileLaunch& L = st.L;
     TileArgs& a = L.args;
-    const int mode = sk_mode_of(L.op, a.N, io);
+    const int mode = sk_mode_of(L.op, a.N, io, (a.flags & TF_BLUE) ? a.n_other : 0);
     if (mode < 0) return;
     const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
     // No compiled kernel for this length: a run-time compiled one (jit.cpp)
@@ -252,7 +253,7 @@ void try_tensor_core(Step& st, const AxisIO& io) {
 }
 
 Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const AxisIO& io, int flags, int rows,
-                    const std::string& what, bool tw4 = false) {
+                    const std::string& what, bool tw4 = false, int blue_n = 0) {
     Step st;
     const long long transforms = io.inner;
     TileShape sh = pick_shape(n, rowlen, column, transforms);
@@ -285,6 +286,7 @@ Step make_tile_step(int op, int sign, int n, int rowlen, bool column, const Axis
     a.out_stride = io.out_stride;
     a.rows = rows;
     a.flags = flags;
+    a.n_other = blue_n;
     a.scale = 1.0f;
     a.div_n = make_fastdiv((uint32_t)std::max(n, 1));
     a.div_p = make_fastdiv((uint32_t)sh.P);
@@ -608,6 +610,35 @@ void add_bluestein(FftPlan& plan, int kind, long long n, long long batch, const 
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " needs Bluestein above 2^22");
     const long long m = bluestein_length(n);
     const int sign = io.sign != 0 ? io.sign : (plan.forward() ? -1 : 1);
+    if (kind == BLUE_C2C && m <= kMaxTileN) {
+        // One size-specialized pulse tile per row does the whole transform:
+        // chirp on load (zero padded to m), convolution, chirp on store
+        // (TF_BLUE); the generic tile kernel has no such form, so without a
+        // specialized kernel the three passes below run instead.
+        AxisIO fio;
+        fio.inner = batch;
+        fio.in_idist = n;
+        fio.out_idist = n;
+        Step st = make_tile_step(OP_PC, 1, (int)m, (int)m, false, fio, TF_BLUE | TF_SCALE, 0,
+                                 "bluestein n=" + std::to_string(n) + " m=" + std::to_string(m), false, (int)n);
+        if (st.sk != nullptr) {
+            st.L.args.mul_pitch_p = 0;
+            st.L.args.mul_pitch_k = 1;
+            st.L.args.scale = io.scale / (float)m;
+            st.batch_dim = 1;
+            st.mul_table = 1;
+            st.tw2_kind = 3;  // the chirp c_j, j < n
+            st.blue_n = n;
+            st.blue_m = m;
+            st.blue_sign = sign;
+            st.src = io.src;
+            st.src_off = io.src_off;
+            st.dst = io.dst;
+            st.dst_off = io.dst_off;
+            plan.steps.push_back(st);
+            return;
+        }
+    }
     const size_t conv = ((size_t)(batch * m * 8) + 255) / 256 * 256;
     Step pre;
     pre.kind = StepKind::Blue;

@@ -64,7 +64,8 @@ struct Step {
     BufPtr mul_buf, chirp_buf;
     PlanDev host_plan{};              // pass list (uploaded to plan_dev)
     std::vector<int> radices;
-    int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count
+    int tw2_kind = 0;                 // 0 none, 1 roots W_n^k for k < count, 2 split cross twiddles,
+                                      // 3 the Bluestein chirp of (blue_n, blue_sign)
     long long tw2_n = 0, tw2_count = 0;
     const SkEntry* sk = nullptr;      // size-specialized kernel, when compiled for this step
     bool tc_cols_in = false, tc_cols_out = false;  // tensor-core step operand layouts

@@ -251,7 +251,8 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
         const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
         sk_copy_run(tid, T, stage, 0, src + (long long)r0 * a.in_idist * 8, (long long)nrows * (K::N / 2 + 1) * 8);
     } else {
-        const int rowlen = K::OP == OP_C2R_HALF ? K::N + 1 : K::N;
+        int rowlen = K::OP == OP_C2R_HALF ? K::N + 1 : K::N;
+        if (K::OP == OP_PC && (a.flags & TF_BLUE)) rowlen = a.n_other;
         sk_copy_run(tid, T, stage, 0, src + c.in_base * 8, (long long)c.cnt * rowlen * 8);
     }
 }
@@ -312,7 +313,13 @@ SIP_HD float2 sk_c2r4a_input(const TileArgs& a, const TileCtx& c, const float2* 
 template <class K>
 SIP_HD float2 sk_input(const TileArgs& a, const TileCtx& c, const float2* stage, int q, int n) {
     constexpr int N = K::N;
-    if constexpr (K::OP == OP_C2C || K::OP == OP_PC) {
+    if constexpr (K::OP == OP_PC) {
+        if (a.flags & TF_BLUE) {  // Bluestein: chirp times the input, zero padded
+            const int nb = a.n_other;
+            return n < nb ? c_mul(stage[q * nb + n], SIP_LDG(a.tw2 + n)) : make_float2(0.f, 0.f);
+        }
+        return stage[q * N + n];
+    } else if constexpr (K::OP == OP_C2C) {
         const float2 v = K::MODE == SK_COLS ? stage[n * K::P + q] : stage[q * N + n];
         return maybe_conj(v, (a.flags & TF_CONJ_IN) != 0);
     } else if constexpr (K::OP == OP_R2C_HALF || K::OP == OP_R2C_4B) {
@@ -449,6 +456,12 @@ struct SkPass {
                     const int k = j + r * NR;
                     float2 v = rg.v[s][r];
                     if constexpr (K::OP == OP_C2C) {
+                        if constexpr (K::WORK_IN) {  // inverse half of a pulse tile
+                            if (a.flags & TF_BLUE) {  // Bluestein: outputs k < n_other times the chirp
+                                if (k >= a.n_other) continue;
+                                v = c_mul(v, SIP_LDG(a.tw2 + k));
+                            }
+                        }
                         if constexpr (K::TW4) v = c_tw<K::SIGN>(v, cross_tw(a, (long long)(c.i0 + q) * k));
                         if (sc) v = c_scale(v, a.scale);
                         v = maybe_conj(v, (a.flags & TF_CONJ_OUT) != 0);
@@ -641,6 +654,22 @@ __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx
     }
 }
 
+// One half of a pulse-compression tile.  SIP_SK_PC_SPLIT = 1 keeps each
+// half out of line, so that it gets its own register allocation instead of
+// one for both halves and the filter between them.
+#ifndef SIP_SK_PC_SPLIT
+#define SIP_SK_PC_SPLIT 0
+#endif
+template <class KV>
+#if SIP_SK_PC_SPLIT
+__device__ __noinline__
+#else
+__device__ __forceinline__
+#endif
+void sk_half(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
+    sk_run<KV, 0>(tid, a, c, buf);
+}
+
 // STAGES = 2: the next tile is staged while the current one is transformed;
 // STAGES = 1: one buffer (tiles too large to double), overlap comes from
 // several CTAs per SM.
@@ -674,10 +703,15 @@ __global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a)
         }
         if constexpr (K::OP == OP_PC) {
             // forward FFT, filter, inverse FFT, all in shared memory
-            sk_run<SkView<K, OP_PC, -1, false>, 0>(tid, a, c, cur);
+            sk_half<SkView<K, OP_PC, -1, false>>(tid, a, c, cur);
             sk_mul<K>(tid, a, c, cur);
             __syncthreads();
-            sk_run<SkView<K, OP_C2C, 1, true>, 0>(tid, a, c, cur);
+            // the inverse half's butterfly indices and addresses equal the
+            // forward half's; an opaque copy of the thread index keeps the
+            // compiler from holding them in registers across both halves
+            int tid_inv = tid;
+            asm volatile("" : "+r"(tid_inv));
+            sk_half<SkView<K, OP_C2C, 1, true>>(tid_inv, a, c, cur);
             __syncthreads();
             continue;
         }

@@ -56,6 +56,9 @@ enum TileFlags : int {
     TF_PLANAR_IN = 32,   // C2C input as two float planes: src (real), src_im (imaginary)
     TF_PLANAR_OUT = 64,  // C2C output as two float planes: dst (real), dst_im (imaginary)
     TF_SHIFT_OUT = 128,  // C2C output rotated per slice of sh_rows x sh_cols (fftshift epilogue)
+    TF_BLUE = 256,    // OP_PC as Bluestein's whole transform (size-specialized tiles only): rows
+                      // of n_other values in and out, times the chirp tw2[j] on load (zero
+                      // padded to N) and tw2[k] on store, outputs k < n_other only
 };
 
 struct TileArgs {

@@ -48,10 +48,23 @@ std::vector<float2> stockham_host(const PlanDev& pd) {
     return t;
 }
 
-// Second table of a step: roots W_n^k (kind 1) or the split cross-twiddle
-// table of four-step passes (kind 2, tile_io.cuh cross_tw).
+// Bluestein chirp c_j = exp(s i pi (j^2 mod 2n) / n), j < n (bluestein.cuh).
+std::vector<float2> chirp_host(long long n, int sign) {
+    std::vector<float2> chirp(n);
+    for (long long j = 0; j < n; ++j) {
+        const long long q = (j * j) % (2 * n);
+        const long double a = 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
+        chirp[j] = make_float2((float)std::cos(a), (float)(sign * std::sin(a)));
+    }
+    return chirp;
+}
+
+// Second table of a step: roots W_n^k (kind 1), the split cross-twiddle
+// table of four-step passes (kind 2, tile_io.cuh cross_tw) or the Bluestein
+// chirp of a fused Bluestein tile (kind 3).
 std::vector<float2> tw2_host(const Step& st) {
     std::vector<float2> t;
+    if (st.tw2_kind == 3) return chirp_host(st.blue_n, st.blue_sign);
     if (st.tw2_kind == 1) {
         for (long long k = 0; k < st.tw2_count; ++k) t.push_back(root_host(k, st.tw2_n));
     } else if (st.tw2_kind == 2) {
@@ -308,13 +321,7 @@ void emu_tc_step(const Step& st, const void* src, void* dst) {
 // Bluestein pre / post pass on the CPU (bluestein.cuh element functions)
 // with the chirp computed on the host.
 void emu_blue_step(const Step& st, const void* src, void* dst) {
-    const long long n = st.blue_n;
-    std::vector<float2> chirp(n);
-    for (long long j = 0; j < n; ++j) {
-        const long long q = (j * j) % (2 * n);
-        const long double a = 3.141592653589793238462643383279502884L * (long double)q / (long double)n;
-        chirp[j] = make_float2((float)std::cos(a), (float)(st.blue_sign * std::sin(a)));
-    }
+    std::vector<float2> chirp = chirp_host(st.blue_n, st.blue_sign);
     BluesteinArgs a = st.blue;
     a.src = src;
     a.dst = dst;
