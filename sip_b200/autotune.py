@@ -7,8 +7,8 @@ elements per thread and radix order (sipFftSetPlanHint).  Each candidate is
 planned, run `warmup` times and timed over `reps` executions with CUDA
 events on device-resident buffers; the fastest is appended to the tune
 cache, the file the planner reads at MakePlan when SIP_FFT_TUNE_CACHE names
-it.  Each line is "type direction dims batch P E generic order fused"
-(dims like 64x128), and the last matching line wins.
+it.  Each line is "type direction dims batch P E generic order fused
+variant jit" (dims like 64x128), and the last matching line wins.
 
 CLI: python -m sip_b200.autotune --type c2c --n 4096 --batch 256 --cache tune.txt
 """
@@ -32,15 +32,17 @@ class Candidate:
     order: int = 0    # radix order (0 descending, 1 ascending)
     fused: int = 0    # real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
     variant: int = 0  # compiled size-specialized variant
+    jit: int = 0      # run-time compiled kernels: 0 default, 1 always, 2 never
 
     def line(self, fft_type: int, direction: int, sizes, batch: int) -> str:
         dims = "x".join(str(int(s)) for s in sizes)
         return (f"{fft_type} {direction} {dims} {batch} {self.p} {self.e} {self.generic} {self.order} "
-                f"{self.fused} {self.variant}\n")
+                f"{self.fused} {self.variant} {self.jit}\n")
 
 
 def candidates(max_p: int = 16) -> list[Candidate]:
     out = [Candidate(), Candidate(fused=1), Candidate(fused=2)] + [Candidate(variant=v) for v in (1, 2, 3)]
+    out += [Candidate(jit=1), Candidate(jit=2)]
     ps = [0] + [p for p in (1, 2, 4, 8, 16, 32) if p <= max_p]
     for p, e, order in itertools.product(ps, (16, 32), (0, 1)):
         out.append(Candidate(p, e, 1, order))
@@ -56,6 +58,7 @@ def apply(handle, c: Candidate) -> None:
     check(handle.set_hint(L.SIP_FFT_HINT_RADIX_ORDER, c.order), "hint order")
     check(handle.set_hint(L.SIP_FFT_HINT_REAL_FUSED, c.fused), "hint real fused")
     check(handle.set_hint(L.SIP_FFT_HINT_SK_VARIANT, c.variant), "hint sk variant")
+    check(handle.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, c.jit), "hint runtime compile")
 
 
 def _buffers(torch, fft_type: int, sizes, batch: int, device):

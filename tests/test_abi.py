@@ -299,6 +299,18 @@ def test_tune_cache_env(tmp_path):
     assert json.loads(r.stdout.strip().splitlines()[-1])[0] is True
 
 
+def test_tune_cache_runtime_compile_field(tmp_path):
+    """The eleventh field of a tune-cache line is the run-time compile hint."""
+    cache = tmp_path / "tune.txt"
+    cache.write_text("16 16 3840 8192 0 0 0 0 0 0 2\n")
+    code = ("import sys,json; sys.path.insert(0, %r); from sip_b200.fft import FftHandle; "
+            "h=FftHandle(); h.make_plan_1d(3840, 0x10, 0x10, 8192); s=h.describe()['steps'][0]; "
+            "print(json.dumps(s['jit']))" % str(ROOT))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       env={**os.environ, "SIP_FFT_TUNE_CACHE": str(cache)})
+    assert json.loads(r.stdout.strip().splitlines()[-1]) is False, r.stderr
+
+
 def test_batch_api_without_device(sip_lib, handle):
     b = ctypes.c_void_p()
     assert sip_lib.sipFftBatchCreate(None) == INV
