@@ -52,9 +52,16 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant
                                            (0 default; a step without that variant uses its default) */
 #define SIP_FFT_HINT_RUNTIME_COMPILE 7  /* steps of a length without a compiled size-specialized
-                                           kernel: 0 default (compile one with NVRTC when the step
-                                           holds >= 2^20 values), 1 always, 2 never (generic kernel) */
+                                           kernel: 0 default (steps of >= 2^20 values use one compiled
+                                           with NVRTC; a configuration not yet compiled is compiled in
+                                           the background and this plan runs the generic kernel),
+                                           1 always, compiled at MakePlan, 2 never (generic kernel) */
 AsdSip::AspbStatus sipFftSetPlanHint(AsdSip::asdFftHandle handle, int key, int value);
+
+/* Waits up to timeout_ms for the run-time kernel compilations started in
+ * the background by MakePlan; ACL_SUCCESS when none is left, else
+ * ACL_ERROR_INTERNAL_ERROR.  No counterpart in the reference.  */
+AsdSip::AspbStatus sipFftJitWait(long long timeout_ms);
 
 /* Compiles (no GPU needed) the run-time specialized kernel the planner
  * would choose for one tile step: op 0 C2C, 1 R2C half-length, 2 C2R

@@ -73,7 +73,7 @@ EXPORTED = [
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
     "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows", "sipFftSetOutputShift",
-    "sipFftJitCompileCheck",
+    "sipFftJitCompileCheck", "sipFftJitWait",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -120,6 +120,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "sipFftExecC2CNoAlloc": (_i32, [_vp, _vp, _vp]),
         "sipFftJitCompileCheck": (_i32, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_longlong]),
+        "sipFftJitWait": (_i32, [ctypes.c_longlong]),
         "sipFftMakePlanPulse1D": (_i32, [_vp, _i64, _i64, _vp, ctypes.c_int]),
         "sipFftBatchAddRows": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
         "sipFftSetOutputShift": (_i32, [_vp, ctypes.c_int, ctypes.c_double]),

@@ -594,6 +594,11 @@ AspbStatus sipFftJitCompileCheck(int op, int mode, int sign, int tw4, int n, lon
     return ACL_SUCCESS;
 }
 
+AspbStatus sipFftJitWait(long long timeout_ms) {
+    if (timeout_ms < 0) return ACL_ERROR_INVALID_PARAM;
+    return sipfft::sk_jit_wait(timeout_ms) ? ACL_SUCCESS : ACL_ERROR_INTERNAL_ERROR;
+}
+
 AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
     std::lock_guard<std::mutex> lk(g_mu);
     FftPlan* p = find_plan(handle);

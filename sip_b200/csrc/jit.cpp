@@ -18,6 +18,9 @@
 #include <mutex>
 #include <sstream>
 #include <thread>
+#include <condition_variable>
+#include <chrono>
+#include <set>
 
 #include "plan.h"
 #include "sk_kernel.cuh"
@@ -300,22 +303,27 @@ int spill_bytes(const std::string& log) {
     return total;
 }
 
-bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err, int* spill) {
+namespace {
+
+// Options, cache key (hash) and cache file of a configuration.
+struct JitKey {
+    std::vector<const char*> opts;
+    std::string hex, path;
+};
+
+JitKey jit_key(const JitCfg& c) {
     const Nvrtc& api = nvrtc();
-    if (!api.ok) {
-        *err = "NVRTC is not available";
-        return false;
-    }
+    JitKey k;
     const std::string src = sk_jit_source();
     const std::string expr = sk_jit_name_expr(c);
     // SIP_FFT_JIT_PC_SPLIT=1: pulse tiles with out-of-line halves (sk_kernel.cuh)
-    std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
-    opts.push_back("--ptxas-options=-v");
-    if (env_int("SIP_FFT_JIT_PC_SPLIT", 0) != 0) opts.push_back("-DSIP_SK_PC_SPLIT=1");
+    k.opts.assign(std::begin(kOptions), std::end(kOptions));
+    k.opts.push_back("--ptxas-options=-v");
+    if (env_int("SIP_FFT_JIT_PC_SPLIT", 0) != 0) k.opts.push_back("-DSIP_SK_PC_SPLIT=1");
     uint64_t h = 1469598103934665603ull;
     const int ver[2] = {api.major, api.minor};
     h = fnv1a(h, ver, sizeof(ver));
-    for (const char* o : opts) h = fnv1a(h, o, std::strlen(o) + 1);
+    for (const char* o : k.opts) h = fnv1a(h, o, std::strlen(o) + 1);
     h = fnv1a(h, src.data(), src.size());
     h = fnv1a(h, expr.data(), expr.size());
     for (int i = 0; i < kJitHeaderCount; ++i) {
@@ -324,11 +332,18 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     }
     char hex[17];
     std::snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)h);
+    k.hex = hex;
     const std::string dir = cache_dir();
-    const std::string path = dir.empty() ? "" : dir + "/sk_" + hex + ".cubin";
+    k.path = dir.empty() ? "" : dir + "/sk_" + k.hex + ".cubin";
+    return k;
+}
+
+// A compiled configuration from the process or disk cache, without compiling.
+bool jit_cached(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, int* spill) {
+    const JitKey k = jit_key(c);
     {
         std::lock_guard<std::mutex> lk(g_jit_mu);
-        auto it = g_jit_cubins.find(hex);
+        auto it = g_jit_cubins.find(k.hex);
         if (it != g_jit_cubins.end()) {
             *cubin = it->second.cubin;
             *lowered = it->second.lowered;
@@ -336,11 +351,29 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
             return true;
         }
     }
-    if (!path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(path, cubin, lowered, spill)) {
+    if (!k.path.empty() && env_int("SIP_FFT_JIT_VERBOSE", 0) == 0 && cache_read(k.path, cubin, lowered, spill)) {
         std::lock_guard<std::mutex> lk(g_jit_mu);
-        g_jit_cubins[hex] = {*cubin, *lowered, *spill};
+        g_jit_cubins[k.hex] = {*cubin, *lowered, *spill};
         return true;
     }
+    return false;
+}
+
+}  // namespace
+
+bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowered, std::string* err, int* spill) {
+    const Nvrtc& api = nvrtc();
+    if (!api.ok) {
+        *err = "NVRTC is not available";
+        return false;
+    }
+    if (jit_cached(c, cubin, lowered, spill)) return true;
+    const std::string src = sk_jit_source();
+    const std::string expr = sk_jit_name_expr(c);
+    const JitKey key = jit_key(c);
+    const std::vector<const char*>& opts = key.opts;
+    const std::string& hex = key.hex;
+    const std::string& path = key.path;
 
     nvrtcProgram prog = nullptr;
     if (api.create(&prog, src.c_str(), "sip_fft_jit.cu", kJitHeaderCount, kJitHeaderTexts, kJitHeaderNames) !=
@@ -386,12 +419,12 @@ bool sk_jit_compile(const JitCfg& c, std::vector<char>* cubin, std::string* lowe
     return true;
 }
 
-bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out,
-                   std::string* err) {
-    // Candidates: at most 32 values per thread and pass (the default), then
-    // 16 and 48, compiled concurrently; the first in that order without
-    // register spills wins, else the one with the fewest spilled bytes.
-    // SIP_FFT_JIT_E pins one.
+namespace {
+
+// Candidate configurations of a step, in order of preference: at most 32
+// values per thread and pass (the default), then 16 and 48.
+// SIP_FFT_JIT_E pins one.
+std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, long long transforms) {
     std::vector<int> tries = {32, 16, 48};
     if (env_int("SIP_FFT_JIT_E", 0) > 0) tries = {env_int("SIP_FFT_JIT_E", 0)};
     std::vector<JitCfg> cands;
@@ -423,6 +456,16 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
             if (ok) add(r);
         }
     }
+    return cands;
+}
+
+}  // namespace
+
+bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out,
+                   std::string* err) {
+    // The candidates are compiled concurrently; the first in order without
+    // register spills wins, else the one with the fewest spilled bytes.
+    const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms);
     if (cands.empty()) {
         *err = "no run-time configuration for this step";
         return false;
@@ -455,26 +498,22 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
     return true;
 }
 
-const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms) {
-    if (!sk_jit_available()) return nullptr;
-    JitCfg c;
-    std::string err;
-    if (!sk_jit_select(op, mode, sign, tw4, n, transforms, &c, &err)) {
-        if (env_int("SIP_FFT_JIT_VERBOSE", 0) != 0) std::fprintf(stderr, "sip_fft jit: %s\n", err.c_str());
-        return nullptr;  // the generic tile kernel runs the step
-    }
+namespace {
+
+// Entry (stable address) of a selected configuration.
+const SkEntry* entry_of(const JitCfg& c) {
     const std::string key = sk_jit_name_expr(c);
     std::lock_guard<std::mutex> lk(g_jit_mu);
     auto it = g_jit_index.find(key);
     if (it != g_jit_index.end()) return it->second;
     SkEntry e;
-    e.n = n;
+    e.n = c.n;
     e.P = c.P;
     e.T = c.T;
-    e.op = op;
-    e.mode = mode;
-    e.sign = sign;
-    e.tw4 = tw4;
+    e.op = c.op;
+    e.mode = c.mode;
+    e.sign = c.sign;
+    e.tw4 = c.tw4;
     e.twb = true;
     e.stages = c.stages;
     e.radices = c.radices;
@@ -488,6 +527,134 @@ const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long lo
     g_jit_entries.push_back(e);
     g_jit_index[key] = &g_jit_entries.back();
     return &g_jit_entries.back();
+}
+
+// Selections by step (the joined candidate names): found + configuration.
+std::map<std::string, std::pair<bool, JitCfg>> g_jit_selected;
+
+// The selection from cached binaries alone, when they decide it: the first
+// candidate without spills whose predecessors are all cached, or the
+// fewest spills when every candidate is cached.
+bool select_cached(const std::vector<JitCfg>& cands, JitCfg* out) {
+    int best = -1, best_spill = 0;
+    for (size_t i = 0; i < cands.size(); ++i) {
+        std::vector<char> cubin;
+        std::string lowered;
+        int spill = 0;
+        if (!jit_cached(cands[i], &cubin, &lowered, &spill)) return false;
+        if (best < 0 || spill < best_spill) {
+            best = (int)i;
+            best_spill = spill;
+        }
+        if (spill == 0) break;
+    }
+    if (best < 0) return false;
+    *out = cands[best];
+    return true;
+}
+
+// Background compilation: a FIFO of steps served by two worker threads,
+// joined when the library unloads.
+struct JitWorkers {
+    std::mutex mu;
+    std::condition_variable cv, idle;
+    std::deque<std::function<void()>> jobs;
+    std::set<std::string> pending;  // step keys queued or running
+    std::vector<std::thread> threads;
+    bool stop = false;
+
+    void start() {  // with mu held
+        if (!threads.empty()) return;
+        for (int i = 0; i < 2; ++i)
+            threads.emplace_back([this] {
+                for (;;) {
+                    std::function<void()> job;
+                    {
+                        std::unique_lock<std::mutex> lk(mu);
+                        cv.wait(lk, [this] { return stop || !jobs.empty(); });
+                        if (stop && jobs.empty()) return;
+                        job = std::move(jobs.front());
+                        jobs.pop_front();
+                    }
+                    job();
+                }
+            });
+    }
+    ~JitWorkers() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+            jobs.clear();
+        }
+        cv.notify_all();
+        for (auto& t : threads) t.join();
+    }
+};
+JitWorkers g_workers;  // after the maps it uses: destroyed (joined) first
+
+}  // namespace
+
+const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms, bool sync) {
+    if (!sk_jit_available()) return nullptr;
+    const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms);
+    if (cands.empty()) return nullptr;
+    std::string step;
+    for (const JitCfg& c : cands) step += sk_jit_name_expr(c) + ";";
+    bool known = false, found = false;
+    JitCfg sel;
+    {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        auto it = g_jit_selected.find(step);
+        if (it != g_jit_selected.end()) {
+            known = true;
+            found = it->second.first;
+            sel = it->second.second;
+        }
+    }
+    if (known) return found ? entry_of(sel) : nullptr;
+    if (select_cached(cands, &sel)) {
+        std::lock_guard<std::mutex> lk(g_jit_mu);
+        g_jit_selected[step] = {true, sel};
+    } else if (sync) {
+        std::string err;
+        const bool ok = sk_jit_select(op, mode, sign, tw4, n, transforms, &sel, &err);
+        if (!ok && env_int("SIP_FFT_JIT_VERBOSE", 0) != 0) std::fprintf(stderr, "sip_fft jit: %s\n", err.c_str());
+        {
+            std::lock_guard<std::mutex> lk(g_jit_mu);
+            g_jit_selected[step] = {ok, sel};
+        }
+        if (!ok) return nullptr;  // the generic tile kernel runs the step
+    } else {
+        // compile in the background; this plan runs the generic kernel, plans
+        // made after the compilation finished use the specialized one
+        std::lock_guard<std::mutex> lk(g_workers.mu);
+        if (!g_workers.stop && g_workers.pending.insert(step).second) {
+            g_workers.jobs.push_back([=] {
+                JitCfg c;
+                std::string err;
+                const bool ok = sk_jit_select(op, mode, sign, tw4, n, transforms, &c, &err);
+                {
+                    std::lock_guard<std::mutex> l2(g_jit_mu);
+                    g_jit_selected[step] = {ok, c};
+                }
+                {
+                    std::lock_guard<std::mutex> l3(g_workers.mu);
+                    g_workers.pending.erase(step);
+                }
+                g_workers.idle.notify_all();
+            });
+            g_workers.start();
+            g_workers.cv.notify_one();
+        }
+        return nullptr;
+    }
+    return entry_of(sel);
+}
+
+bool sk_jit_wait(long long timeout_ms) {
+    std::unique_lock<std::mutex> lk(g_workers.mu);
+    return g_workers.idle.wait_for(lk, std::chrono::milliseconds(std::max(0LL, timeout_ms)),
+                                   [] { return g_workers.pending.empty(); });
 }
 
 const void* sk_jit_load(const SkEntry* entry) {

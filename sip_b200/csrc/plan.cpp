@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <functional>
 #include <map>
 #include <sstream>
@@ -211,8 +212,13 @@ void try_specialize(Step& st, const AxisIO& io) {
     // No compiled kernel for this length: a run-time compiled one (jit.cpp)
     // for steps large enough to repay the compilation, or on request.
     const long long values = io.inner * io.outer * (long long)a.N;
-    if (e == nullptr && (g_hint_jit == 1 || (g_hint_jit == 0 && values >= (1LL << 20))))
-        e = sk_jit_entry(L.op, mode, L.sign, L.tw4, a.N, io.inner);
+    if (e == nullptr && (g_hint_jit == 1 || (g_hint_jit == 0 && values >= (1LL << 20)))) {
+        // hint 1 (or SIP_FFT_JIT_SYNC=1) compiles now; the default compiles
+        // a new configuration in the background and plans later shapes with it
+        const char* sync_env = std::getenv("SIP_FFT_JIT_SYNC");
+        const bool sync = g_hint_jit == 1 || (sync_env != nullptr && std::strcmp(sync_env, "1") == 0);
+        e = sk_jit_entry(L.op, mode, L.sign, L.tw4, a.N, io.inner, sync);
+    }
     if (e == nullptr) return;
     st.sk = e;
     st.radices = e->radices;

@@ -29,10 +29,15 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant 
 const std::vector<SkEntry>& sk_registry();
 
 // Run-time specialization (jit.cpp): an entry for a configuration that
-// sk_configs.h does not compile, chosen from (op, mode, n, transforms);
-// its kernel is compiled by NVRTC when the plan is first prepared on a
-// device.  nullptr when no configuration fits or NVRTC is not available.
-const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms);
+// sk_configs.h does not compile, chosen from (op, mode, n, transforms) and
+// compiled by NVRTC (loaded when the plan is first prepared on a device).
+// Not yet compiled: `sync` compiles it now, else it is compiled in the
+// background and nullptr returned (the generic kernel runs this step; plans
+// made later get the entry).  nullptr also when no configuration fits or
+// NVRTC is not available.
+const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long long transforms, bool sync);
 bool sk_jit_available();
+// Waits up to timeout_ms for the background compilations; true when none is left.
+bool sk_jit_wait(long long timeout_ms);
 
 }  // namespace sipfft

@@ -205,8 +205,9 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant)
     return first;
 }
 // The harness runs only the kernels it instantiates: no run-time compiled ones.
-const SkEntry* sk_jit_entry(int, int, int, bool, int, long long) { return nullptr; }
+const SkEntry* sk_jit_entry(int, int, int, bool, int, long long, bool) { return nullptr; }
 bool sk_jit_available() { return false; }
+bool sk_jit_wait(long long) { return true; }
 }  // namespace sipfft
 
 namespace {

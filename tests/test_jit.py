@@ -58,6 +58,13 @@ def test_planner_choice(op, direction, n, batch, jit, expect):
     h = _plan(op, direction, [n], batch, jit)
     steps = [s for s in h.describe()["steps"] if "jit" in s]
     h.destroy()
+    if jit == 0 and expect:
+        # the default compiles a new configuration in the background: this
+        # plan may run the generic kernel, one made after the wait does not
+        assert L.lib().sipFftJitWait(300000) == L.ACL_SUCCESS
+        h = _plan(op, direction, [n], batch, jit)
+        steps = [s for s in h.describe()["steps"] if "jit" in s]
+        h.destroy()
     assert any(s["jit"] for s in steps) == expect, steps
     for s in steps:
         if s["jit"]:
@@ -68,6 +75,7 @@ def test_planner_choice(op, direction, n, batch, jit, expect):
 def test_hint_validation():
     from sip_b200.fft import FftHandle
 
+    assert L.lib().sipFftJitWait(-1) == L.ACL_ERROR_INVALID_PARAM
     h = FftHandle()
     assert h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, 3) == L.ACL_ERROR_INVALID_PARAM
     assert h.set_hint(L.SIP_FFT_HINT_RUNTIME_COMPILE, 2) == L.ACL_SUCCESS
@@ -226,3 +234,36 @@ def test_jit_bluestein(cuda, jit_cache, op, direction, n, batch):
     assert used
     err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
     assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+
+
+def _random_lengths(seed, count):
+    """Lengths up to one tile whose factors are all <= 31 and that have no
+    compiled kernel, drawn with a fixed seed."""
+    rng = np.random.default_rng(seed)
+    primes = [2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31]
+    compiled = {50, 256, 500, 1000, 1024, 2048, 2187, 3000, 4096, 6000, 8192}
+    out = []
+    while len(out) < count:
+        n = 1
+        for _ in range(int(rng.integers(2, 6))):
+            n *= int(rng.choice(primes, p=[.3, .2, .15, .1, .05, .05, .05, .04, .02, .02, .02]))
+        if 64 <= n <= 16384 and n not in compiled and n not in out:
+            out.append(n)
+    return out
+
+
+# Randomly drawn lengths with the run-time kernels forced on: C2C rows both
+# directions, R2C / C2R (half length for even n, row pairs for odd n).
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", _random_lengths(20261203, 12))
+@pytest.mark.parametrize("op,direction", [(O.C2C, O.FORWARD), (O.C2C, O.INVERSE), (O.R2C, O.FORWARD),
+                                          (O.C2R, O.INVERSE)])
+def test_jit_random_lengths(cuda, jit_cache, n, op, direction):
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    batch = 7
+    x = _input(op, [n], batch, seed=n + op)
+    out, used = _gpu(cuda, op, direction, [n], batch, x, jit=1)
+    assert used
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, f"n={n} rel_l2 vs FP64 {err:.3e}"
