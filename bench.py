@@ -682,7 +682,16 @@ def run_ours(args) -> None:
         published = published_configs(torch, dev, stream)
     serve = None
     if rank == 0 and not args.no_serve:
-        serve = serving(torch, args.serve_requests)
+        # Both serving paths run the generic tile kernels (the queue's kernels
+        # are generic by design): the plain path plans every new (N, batch),
+        # and background compilation of run-time kernels for hundreds of
+        # request shapes would compete with the serving loop for host cores.
+        os.environ["SIP_FFT_JIT"] = "0"
+        try:
+            serve = serving(torch, args.serve_requests)
+            serve["runtime_kernels"] = "off (SIP_FFT_JIT=0) for both paths"
+        finally:
+            os.environ.pop("SIP_FFT_JIT", None)
 
     if dist:
         dist.barrier()

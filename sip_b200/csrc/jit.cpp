@@ -248,6 +248,23 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     c.tw4 = tw4;
     c.n = n;
     c.radices = jit_radices(n);
+    // Tuning overrides (sweeps; unset in normal use): SIP_FFT_JIT_RADICES
+    // ("25,15,8", must multiply to n), SIP_FFT_JIT_P, SIP_FFT_JIT_T,
+    // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES.
+    if (const char* rs = std::getenv("SIP_FFT_JIT_RADICES")) {
+        std::vector<int> r;
+        long long prod = 1;
+        for (const char* q = rs; *q;) {
+            const int v = std::atoi(q);
+            if (v < 2 || v > 32) return false;
+            r.push_back(v);
+            prod *= v;
+            while (*q && *q != ',') ++q;
+            if (*q == ',') ++q;
+        }
+        if (prod != n || r.empty() || r.size() > (size_t)kMaxPasses) return false;
+        c.radices = r;
+    }
     if (c.radices.empty()) return false;
     transforms = std::max<long long>(1, transforms);
     // transforms per tile: about SIP_FFT_JIT_TILE (4096) values for rows,
@@ -265,6 +282,9 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
         P = std::max<long long>(1, P / 2);
     }
     if (T > kMaxTileThreads) return false;
+    if (env_int("SIP_FFT_JIT_P", 0) > 0) P = std::min<long long>(env_int("SIP_FFT_JIT_P", 0), transforms);
+    if (env_int("SIP_FFT_JIT_T", 0) > 0) T = env_int("SIP_FFT_JIT_T", 0);
+    if (T % 32 != 0 || T > kMaxTileThreads) return false;
     c.P = (int)P;
     c.T = T;
     const int r0 = c.radices[0];
@@ -273,9 +293,11 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     if (2 * buf <= kMaxTileSmem) c.stages = 2;
     else if (buf <= kMaxTileSmem) c.stages = 1;
     else return false;
+    if (env_int("SIP_FFT_JIT_STAGES", 0) == 1) c.stages = 1;
     c.smem = (int)(c.stages * buf);
     const int smem_ctas = std::max<int>(1, (228 * 1024) / (c.smem + 1024));
     c.minb = std::max(1, std::min(65536 / (T * 128), smem_ctas));
+    if (env_int("SIP_FFT_JIT_MINB", 0) > 0) c.minb = env_int("SIP_FFT_JIT_MINB", 0);
     *out = c;
     return true;
 }

@@ -208,7 +208,11 @@ void try_specialize(Step& st, const AxisIO& io) {
     TileArgs& a = L.args;
     const int mode = sk_mode_of(L.op, a.N, io, (a.flags & TF_BLUE) ? a.n_other : 0);
     if (mode < 0) return;
-    const SkEntry* e = sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
+    // SIP_FFT_JIT_PREFER=1 (tuning sweeps) skips the compiled kernels so that
+    // run-time configurations can be timed against them
+    const char* prefer = std::getenv("SIP_FFT_JIT_PREFER");
+    const bool prefer_jit = prefer != nullptr && std::strcmp(prefer, "1") == 0;
+    const SkEntry* e = prefer_jit ? nullptr : sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
     // No compiled kernel for this length: a run-time compiled one (jit.cpp)
     // for steps large enough to repay the compilation, or on request.
     const long long values = io.inner * io.outer * (long long)a.N;
