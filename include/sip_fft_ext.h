@@ -52,7 +52,7 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant
                                            (0 default; a step without that variant uses its default) */
 #define SIP_FFT_HINT_RUNTIME_COMPILE 7  /* steps of a length without a compiled size-specialized
-                                           kernel: 0 default (steps of >= 2^20 values use one compiled
+                                           kernel: 0 default (steps of >= 2^18 values use one compiled
                                            with NVRTC; a configuration not yet compiled is compiled in
                                            the background and this plan runs the generic kernel),
                                            1 always, compiled at MakePlan, 2 never (generic kernel) */

@@ -216,7 +216,7 @@ void try_specialize(Step& st, const AxisIO& io) {
     // No compiled kernel for this length: a run-time compiled one (jit.cpp)
     // for steps large enough to repay the compilation, or on request.
     const long long values = io.inner * io.outer * (long long)a.N;
-    if (e == nullptr && (g_hint_jit == 1 || (g_hint_jit == 0 && values >= (1LL << 20)))) {
+    if (e == nullptr && (g_hint_jit == 1 || (g_hint_jit == 0 && values >= (1LL << 18)))) {
         // hint 1 (or SIP_FFT_JIT_SYNC=1) compiles now; the default compiles
         // a new configuration in the background and plans later shapes with it
         const char* sync_env = std::getenv("SIP_FFT_JIT_SYNC");
