@@ -2,6 +2,7 @@
 #include "jit.h"
 
 #include <dlfcn.h>
+#include <pthread.h>
 #include <nvrtc.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -16,6 +17,7 @@
 #include <functional>
 #include <map>
 #include <mutex>
+#include <new>
 #include <sstream>
 #include <thread>
 #include <condition_variable>
@@ -143,16 +145,18 @@ int jit_threads(int P, int n, const std::vector<int>& radices, int e) {
 }
 
 // ------------------------------------------------------------ registry
-std::mutex g_jit_mu;
-std::deque<SkEntry> g_jit_entries;  // stable addresses
-std::map<std::string, SkEntry*> g_jit_index;
-std::map<std::string, const void*> g_jit_kernels;  // name expression -> loaded kernel
+// Registry state lives on the heap and is never destroyed: background
+// compilations may still run while the process exits.
+std::mutex& g_jit_mu = *new std::mutex;
+std::deque<SkEntry>& g_jit_entries = *new std::deque<SkEntry>;  // stable addresses
+std::map<std::string, SkEntry*>& g_jit_index = *new std::map<std::string, SkEntry*>;
+std::map<std::string, const void*>& g_jit_kernels = *new std::map<std::string, const void*>;  // name -> kernel
 struct JitBinary {
     std::vector<char> cubin;
     std::string lowered;
     int spill = 0;
 };
-std::map<std::string, JitBinary> g_jit_cubins;  // cache key -> compiled in this process
+std::map<std::string, JitBinary>& g_jit_cubins = *new std::map<std::string, JitBinary>;  // key -> compiled here
 
 JitCfg cfg_of(const SkEntry& e) {
     JitCfg c;
@@ -228,7 +232,14 @@ void cache_write(const std::string& path, const std::vector<char>& cubin, const 
 
 }  // namespace
 
+// Set in a child process forked from one that had started the compiler's
+// worker threads: the compiler's state may have been copied in the middle
+// of a compilation by another thread, so the child does not compile (its
+// plans run the generic or compiled kernels).
+static bool g_forked_child = false;
+
 bool sk_jit_available() {
+    if (g_forked_child) return false;
     const char* env = std::getenv("SIP_FFT_JIT");
     if (env != nullptr && std::strcmp(env, "0") == 0) return false;
     return nvrtc().ok;
@@ -552,7 +563,7 @@ const SkEntry* entry_of(const JitCfg& c) {
 }
 
 // Selections by step (the joined candidate names): found + configuration.
-std::map<std::string, std::pair<bool, JitCfg>> g_jit_selected;
+std::map<std::string, std::pair<bool, JitCfg>>& g_jit_selected = *new std::map<std::string, std::pair<bool, JitCfg>>;
 
 // The selection from cached binaries alone, when they decide it: the first
 // candidate without spills whose predecessors are all cached, or the
@@ -575,44 +586,109 @@ bool select_cached(const std::vector<JitCfg>& cands, JitCfg* out) {
     return true;
 }
 
-// Background compilation: a FIFO of steps served by two worker threads,
-// joined when the library unloads.
+// Background compilation: a FIFO of steps served by two detached worker
+// threads.  The state is never destroyed, so a worker still compiling while
+// the process exits touches no destroyed object; an exit handler (registered
+// after NVRTC is loaded, so it runs before NVRTC's own teardown) stops the
+// queue and waits up to 30 s for the jobs already running.  A fork waits
+// (up to 60 s) until no compilation is running, so that no compiler state
+// is copied mid-compilation; the child starts with an empty queue and no
+// workers (its parent's threads do not exist there), re-creates its locks
+// and compiles nothing (g_forked_child).
+void register_drain();
+
 struct JitWorkers {
     std::mutex mu;
     std::condition_variable cv, idle;
     std::deque<std::function<void()>> jobs;
     std::set<std::string> pending;  // step keys queued or running
-    std::vector<std::thread> threads;
-    bool stop = false;
+    int running = 0;                // jobs being run
+    bool started = false, stop = false;
 
     void start() {  // with mu held
-        if (!threads.empty()) return;
+        if (started) return;
+        started = true;
         for (int i = 0; i < 2; ++i)
-            threads.emplace_back([this] {
+            std::thread([this] {
                 for (;;) {
                     std::function<void()> job;
                     {
                         std::unique_lock<std::mutex> lk(mu);
                         cv.wait(lk, [this] { return stop || !jobs.empty(); });
-                        if (stop && jobs.empty()) return;
+                        if (stop) return;
                         job = std::move(jobs.front());
                         jobs.pop_front();
+                        ++running;
                     }
+                    // exit handlers run last-registered first: registering the
+                    // drain again here puts it ahead of any handler the
+                    // compiler registered during earlier compilations
+                    register_drain();
                     job();
+                    job = nullptr;
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        --running;
+                    }
+                    idle.notify_all();
                 }
-            });
-    }
-    ~JitWorkers() {
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            stop = true;
-            jobs.clear();
-        }
-        cv.notify_all();
-        for (auto& t : threads) t.join();
+            }).detach();
     }
 };
-JitWorkers g_workers;  // after the maps it uses: destroyed (joined) first
+
+JitWorkers& workers();
+void drain_at_exit();
+
+void register_drain() { std::atexit(&drain_at_exit); }
+
+void drain_at_exit() {
+    JitWorkers& w = workers();
+    std::unique_lock<std::mutex> lk(w.mu);
+    w.stop = true;
+    w.jobs.clear();
+    w.cv.notify_all();
+    w.idle.wait_for(lk, std::chrono::seconds(30), [&w] { return w.running == 0; });
+}
+
+// Fork: no compilation may be in flight; the lock is held across the fork.
+void before_fork() {
+    JitWorkers& w = workers();
+    w.mu.lock();
+    for (int i = 0; i < 600 && w.running > 0; ++i) {
+        w.mu.unlock();
+        std::this_thread::sleep_for(std::chrono::milliseconds(100));
+        w.mu.lock();
+    }
+}
+
+void after_fork_parent() {
+    workers().mu.unlock();
+    register_drain();
+}
+
+void after_fork_child() {
+    JitWorkers& w = workers();
+    new (&w.mu) std::mutex;
+    new (&w.cv) std::condition_variable;
+    new (&w.idle) std::condition_variable;
+    w.jobs.clear();
+    w.pending.clear();
+    w.running = 0;
+    w.started = false;
+    w.stop = false;
+    new (&g_jit_mu) std::mutex;
+    g_forked_child = true;
+}
+
+JitWorkers& workers() {
+    static JitWorkers* w = [] {
+        JitWorkers* p = new JitWorkers;
+        pthread_atfork(&before_fork, &after_fork_parent, &after_fork_child);
+        register_drain();
+        return p;
+    }();
+    return *w;
+}
 
 }  // namespace
 
@@ -649,9 +725,10 @@ const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long lo
     } else {
         // compile in the background; this plan runs the generic kernel, plans
         // made after the compilation finished use the specialized one
-        std::lock_guard<std::mutex> lk(g_workers.mu);
-        if (!g_workers.stop && g_workers.pending.insert(step).second) {
-            g_workers.jobs.push_back([=] {
+        JitWorkers& w = workers();
+        std::lock_guard<std::mutex> lk(w.mu);
+        if (!w.stop && w.pending.insert(step).second) {
+            w.jobs.push_back([=] {
                 JitCfg c;
                 std::string err;
                 const bool ok = sk_jit_select(op, mode, sign, tw4, n, transforms, &c, &err);
@@ -660,13 +737,13 @@ const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long lo
                     g_jit_selected[step] = {ok, c};
                 }
                 {
-                    std::lock_guard<std::mutex> l3(g_workers.mu);
-                    g_workers.pending.erase(step);
+                    std::lock_guard<std::mutex> l3(workers().mu);
+                    workers().pending.erase(step);
                 }
-                g_workers.idle.notify_all();
+                workers().idle.notify_all();
             });
-            g_workers.start();
-            g_workers.cv.notify_one();
+            w.start();
+            w.cv.notify_one();
         }
         return nullptr;
     }
@@ -674,9 +751,10 @@ const SkEntry* sk_jit_entry(int op, int mode, int sign, bool tw4, int n, long lo
 }
 
 bool sk_jit_wait(long long timeout_ms) {
-    std::unique_lock<std::mutex> lk(g_workers.mu);
-    return g_workers.idle.wait_for(lk, std::chrono::milliseconds(std::max(0LL, timeout_ms)),
-                                   [] { return g_workers.pending.empty(); });
+    JitWorkers& w = workers();
+    std::unique_lock<std::mutex> lk(w.mu);
+    return w.idle.wait_for(lk, std::chrono::milliseconds(std::max(0LL, timeout_ms)),
+                           [&w] { return w.pending.empty(); });
 }
 
 const void* sk_jit_load(const SkEntry* entry) {

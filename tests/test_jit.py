@@ -267,3 +267,41 @@ def test_jit_random_lengths(cuda, jit_cache, n, op, direction):
     assert used
     err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
     assert err <= REL_L2_TOL, f"n={n} rel_l2 vs FP64 {err:.3e}"
+
+
+def test_background_compile_exit_and_fork(tmp_path):
+    """A process may exit while a background compilation runs, and a child
+    forked while the compiler's worker threads exist (their state may have
+    been copied mid-compilation) compiles nothing: its plans run the generic
+    kernel, and the parent goes on compiling."""
+    import subprocess
+    import sys
+
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    code = r'''
+import os, sys
+sys.path.insert(0, %r)
+from sip_b200 import _lib as L
+from sip_b200.fft import FftHandle
+def plan(n):
+    h = FftHandle()
+    assert h.make_plan_1d(n, L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, 4096) == 0
+    jit = any(s.get("jit") for s in h.describe()["steps"])
+    h.destroy()
+    return jit
+plan(3780)                      # starts the workers and a background compilation
+pid = os.fork()
+if pid == 0:
+    ok = not plan(3960) and L.lib().sipFftJitWait(1000) == 0 and not plan(3960)
+    os._exit(0 if ok else 3)
+_, status = os.waitpid(pid, 0)
+assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0, status
+plan(4200)
+assert L.lib().sipFftJitWait(300000) == 0 and plan(4200)
+plan(4320)                      # leave one running at exit
+''' % os.getcwd()
+    env = dict(os.environ, SIP_FFT_JIT_CACHE=str(tmp_path / "jit"))
+    r = subprocess.run([sys.executable, "-W", "ignore", "-c", code], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
