@@ -138,6 +138,12 @@ int even_ld(int rowlen) {
 
 constexpr int kSmemLimit = kMaxTileSmem;
 constexpr int kRowTileBytes = 64 * 1024;
+// Row tiles of the generic kernel hold about this many values: small CTAs
+// (32-256 threads at 32 values per thread), several per SM, so that one
+// CTA's loads overlap another's passes (the generic kernel does not stage
+// the next tile itself).  Measured against 16 values per thread and 64 KB
+// tiles: 11-31 % faster on C2C 544 to 6720, R2C 6688, C2R 3000.
+constexpr int kRowTileValues = 2048;
 
 struct TileShape {
     int e, P, T, LD, smem;
@@ -147,7 +153,7 @@ struct TileShape {
 // store side, so P sets the contiguous run length (8-16 values wanted).
 TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     TileShape s{};
-    s.e = (n > 8192 || (column && n >= 1024)) ? 32 : 16;
+    s.e = 32;
     if (g_hint_e == 16 && n <= 8192) s.e = 16;
     if (g_hint_e == 32) s.e = 32;
     s.LD = even_ld(std::max(rowlen, 1));
@@ -157,7 +163,8 @@ TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     if (column) {
         p = std::min<long long>({16, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
     } else {
-        p = std::min<long long>(maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes));
+        p = std::min<long long>({maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes),
+                                 std::max<long long>(1, kRowTileValues / std::max(n, 1))});
     }
     if (g_hint_p > 0)
         p = std::min<long long>({(long long)g_hint_p, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
