@@ -142,7 +142,11 @@ constexpr int kRowTileBytes = 64 * 1024;
 // (32-256 threads at 32 values per thread), several per SM, so that one
 // CTA's loads overlap another's passes (the generic kernel does not stage
 // the next tile itself).  Measured against 16 values per thread and 64 KB
-// tiles: 11-31 % faster on C2C 544 to 6720, R2C 6688, C2R 3000.
+// tiles: 11-31 % faster on C2C 544 to 6720, R2C 6688, C2R 3000.  Plans made
+// with the generic-only hint keep 64 KB tiles and 16 values per thread up
+// to N = 8192: the batch work queue (queue.cu), which runs those plans,
+// gives every tile a 512-thread CTA and claims tiles one by one, and
+// lost 20 % of its serving capacity with the small tiles.
 constexpr int kRowTileValues = 2048;
 
 struct TileShape {
@@ -153,7 +157,8 @@ struct TileShape {
 // store side, so P sets the contiguous run length (8-16 values wanted).
 TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     TileShape s{};
-    s.e = 32;
+    const bool queue_shape = g_hint_generic != 0;
+    s.e = queue_shape ? ((n > 8192 || (column && n >= 1024)) ? 32 : 16) : 32;
     if (g_hint_e == 16 && n <= 8192) s.e = 16;
     if (g_hint_e == 32) s.e = 32;
     s.LD = even_ld(std::max(rowlen, 1));
@@ -163,8 +168,8 @@ TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     if (column) {
         p = std::min<long long>({16, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
     } else {
-        p = std::min<long long>({maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes),
-                                 std::max<long long>(1, kRowTileValues / std::max(n, 1))});
+        p = std::min<long long>(maxp_thr, std::max<long long>(1, kRowTileBytes / row_bytes));
+        if (!queue_shape) p = std::min<long long>(p, std::max<long long>(1, kRowTileValues / std::max(n, 1)));
     }
     if (g_hint_p > 0)
         p = std::min<long long>({(long long)g_hint_p, maxp_thr, std::max<long long>(1, kSmemLimit / row_bytes)});
