@@ -143,10 +143,10 @@ constexpr int kRowTileBytes = 64 * 1024;
 // CTA's loads overlap another's passes (the generic kernel does not stage
 // the next tile itself).  Measured against 16 values per thread and 64 KB
 // tiles: 11-31 % faster on C2C 544 to 6720, R2C 6688, C2R 3000.  Plans made
-// with the generic-only hint keep 64 KB tiles and 16 values per thread up
-// to N = 8192: the batch work queue (queue.cu), which runs those plans,
-// gives every tile a 512-thread CTA and claims tiles one by one, and
-// lost 20 % of its serving capacity with the small tiles.
+// with the generic-only hint keep 64 KB tiles (still at 32 values per
+// thread): the batch work queue (queue.cu), which runs those plans, gives
+// every tile a 512-thread CTA and claims tiles one by one, and lost 20 % of
+// its serving capacity with the small tiles.
 constexpr int kRowTileValues = 2048;
 
 struct TileShape {
@@ -158,7 +158,7 @@ struct TileShape {
 TileShape pick_shape(int n, int rowlen, bool column, long long transforms) {
     TileShape s{};
     const bool queue_shape = g_hint_generic != 0;
-    s.e = queue_shape ? ((n > 8192 || (column && n >= 1024)) ? 32 : 16) : 32;
+    s.e = 32;
     if (g_hint_e == 16 && n <= 8192) s.e = 16;
     if (g_hint_e == 32) s.e = 32;
     s.LD = even_ld(std::max(rowlen, 1));
