@@ -172,6 +172,7 @@ JitCfg cfg_of(const SkEntry& e) {
     c.radices = e.radices;
     c.LD = e.LD;
     c.smem = e.smem;
+    c.twb = e.twb ? 1 : 0;
     return c;
 }
 
@@ -261,7 +262,8 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     c.radices = jit_radices(n);
     // Tuning overrides (sweeps; unset in normal use): SIP_FFT_JIT_RADICES
     // ("25,15,8", must multiply to n), SIP_FFT_JIT_P, SIP_FFT_JIT_T,
-    // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES.
+    // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES, SIP_FFT_JIT_TWB (0: full twiddle
+    // table instead of the basis table).
     if (const char* rs = std::getenv("SIP_FFT_JIT_RADICES")) {
         std::vector<int> r;
         long long prod = 1;
@@ -309,6 +311,7 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     const int smem_ctas = std::max<int>(1, (228 * 1024) / (c.smem + 1024));
     c.minb = std::max(1, std::min(65536 / (T * 128), smem_ctas));
     if (env_int("SIP_FFT_JIT_MINB", 0) > 0) c.minb = env_int("SIP_FFT_JIT_MINB", 0);
+    if (env_int("SIP_FFT_JIT_TWB", 1) == 0) c.twb = 0;
     *out = c;
     return true;
 }
@@ -318,7 +321,7 @@ std::string sk_jit_source() { return "#include \"sk_kernel.cuh\"\n"; }
 std::string sk_jit_name_expr(const JitCfg& c) {
     std::ostringstream s;
     s << "&sipfft::sk_fft_kernel<sipfft::SkCfg<" << c.n << ", " << c.P << ", " << c.T << ", " << c.op << ", "
-      << c.mode << ", " << c.sign << ", " << (c.tw4 ? "true" : "false") << ", " << c.minb << ", 1";
+      << c.mode << ", " << c.sign << ", " << (c.tw4 ? "true" : "false") << ", " << c.minb << ", " << c.twb;
     for (int r : c.radices) s << ", " << r;
     s << ">, " << c.stages << ">";
     return s.str();
@@ -547,7 +550,7 @@ const SkEntry* entry_of(const JitCfg& c) {
     e.mode = c.mode;
     e.sign = c.sign;
     e.tw4 = c.tw4;
-    e.twb = true;
+    e.twb = c.twb != 0;
     e.stages = c.stages;
     e.radices = c.radices;
     e.LD = c.LD;

@@ -31,6 +31,7 @@ struct JitCfg {
     int n = 0, P = 1, T = 32, stages = 2, minb = 1;
     std::vector<int> radices;
     int LD = 0, smem = 0;
+    int twb = 1;  // pass twiddles: 1 basis table, 0 full Stockham table (SkCfg TWB)
 };
 
 // Host-side configuration for at most `values` values per thread and pass
