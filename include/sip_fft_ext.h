@@ -142,11 +142,14 @@ AsdSip::AspbStatus sipFftBatchTakeStatus(sipFftBatch batch, unsigned* status);
  * would exceed 32 MiB (batch x length > 4,194,304 complex points for a
  * two-pass length) gives ACL_ERROR_INVALID_PARAM with a message; a non-C2C
  * or tensor-core plan gives ACL_ERROR_API_NOT_SUPPORT.  Runs on the plan's
- * device and stream.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  Every call shares the array, so calls whose kernels overlap on
- * the GPU race: order them, e.g. on one stream.  No counterpart in the
- * reference. */
+ * device and stream.  The array's device address is looked up
+ * (cudaGetSymbolAddress) when MakePlan prepares an eligible plan on its
+ * device; under CUDA's default lazy module loading that is also when the
+ * array is reserved, so the exec call itself loads and reserves nothing.
+ * Make the plan before any stream capture, and make new plans after a
+ * cudaDeviceReset.  Every call shares the array, so calls whose kernels
+ * overlap on the GPU race: order them, e.g. on one stream.  No counterpart
+ * in the reference. */
 AsdSip::AspbStatus sipFftExecC2CNoAlloc(AsdSip::asdFftHandle handle, const void* input, void* output);
 
 /* Library version string. */

@@ -797,8 +797,10 @@ AspbStatus sipFftExecC2CNoAlloc(asdFftHandle handle, const void* input, void* ou
         std::fprintf(stderr, "[sip_b200] input and output overlap\n");
         return ACL_ERROR_INVALID_PARAM;
     }
-    if (!device_present() || !p->resources_ready) {
-        std::fprintf(stderr, "[sip_b200] no-alloc exec: the plan has no device tables (no GPU at plan time)\n");
+    if (!device_present() || !p->resources_ready || p->noalloc_scratch == nullptr) {
+        std::fprintf(stderr,
+                     "[sip_b200] no-alloc exec: the plan was not prepared on a device (no GPU at plan time, or the "
+                     "static scratch could not be looked up)\n");
         return ACL_ERROR_INTERNAL_ERROR;
     }
     DeviceGuard g(p->device);

@@ -42,6 +42,13 @@ dim3 grid2(long long per_row, long long rows) {
 
 }  // namespace
 
+cudaError_t bluestein_prepare() {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_blue_pre);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_blue_post);
+    return e;
+}
+
 cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream) {
     k_blue_pre<<<grid2(a.m, a.rows), kBlueBlock, 0, stream>>>(a);
     return cudaGetLastError();

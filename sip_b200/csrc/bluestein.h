@@ -11,6 +11,9 @@ namespace sipfft {
 
 cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream);
 cudaError_t bluestein_post(const BluesteinArgs& a, cudaStream_t stream);
+// Queries both pass kernels, which loads their module under lazy loading
+// (plan time, so that an exec does not load code).
+cudaError_t bluestein_prepare();
 
 // Chirp c_j = exp(sign i pi (j^2 mod 2n) / n), j < n (FP64, rounded once).
 cudaError_t gen_chirp(float2* out, long long n, int sign, cudaStream_t stream);

@@ -6,12 +6,14 @@
 // core/fft/utils/fftensor_cache.cpp:82-101).
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <sstream>
 #include <tuple>
 
 #include "jit.h"
+#include "noalloc.h"
 #include "plan.h"
 #include "tc_core.cuh"
 #include "tc_launch.h"
@@ -154,13 +156,27 @@ BufPtr blue_filter_table(int device, long long n, long long m, int sign) {
 
 }  // namespace
 
+ChunkLanes::~ChunkLanes() {
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (side) cudaStreamDestroy(side);
+}
+
 void prepare_device(FftPlan& plan) {
     int device = -1;
     check(cudaGetDevice(&device), "cudaGetDevice");
+    if (!plan.chunk_groups.empty()) {
+        auto l = std::make_shared<ChunkLanes>();
+        check(cudaStreamCreateWithFlags(&l->side, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventCreateWithFlags(&l->join, cudaEventDisableTiming), "cudaEventCreate");
+        plan.lanes = l;
+    }
     for (Step& st : plan.steps) {
         if (st.kind == StepKind::Blue) {
             st.chirp_buf = chirp_table(device, st.blue_n, st.blue_sign);
             st.blue.chirp = static_cast<const float2*>(st.chirp_buf->ptr);
+            check(bluestein_prepare(), "bluestein_prepare");
             continue;
         }
         if (st.mul_table == 1) {
@@ -202,12 +218,16 @@ void prepare_device(FftPlan& plan) {
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
             const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
             st.L.grid = (int)std::min<long long>(st.L.args.ntiles, resident);
+            st.max_grid = (int)std::min<long long>(resident, 0x7fffffffLL);
             st.L.sk_fn = fn;
         } else {
             check(tile_prepare(st.L.sign, st.L.e, st.L.op, st.L.tw4, st.L.smem_bytes), "cudaFuncSetAttribute");
         }
     }
     plan.device = device;
+    // the static scratch of the no-alloc exec is looked up (and, under lazy
+    // module loading, reserved) here rather than in that exec call
+    noalloc_resolve(plan);
     plan.resources_ready = true;
 }
 
@@ -221,8 +241,13 @@ void launch_separated(const FftPlan& plan, const float* in_re, const float* in_i
     check(tile_launch(L, in_re, out_re, static_cast<cudaStream_t>(plan.stream)), "tile kernel launch");
 }
 
-void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
-    cudaStream_t stream = static_cast<cudaStream_t>(plan.stream);
+namespace {
+
+// Launches one step, restricted to chunk units [u0, u0 + cnt) of its chunk
+// group on lane `lane` (cu units per chunk) when cnt >= 0 (cnt < 0: the whole
+// step as planned).
+void launch_one(const Step& st, cudaStream_t stream, const void* in, void* out, void* ws, long long u0,
+                long long cnt, int lane = 0, long long cu = 0) {
     auto resolve = [&](Loc l, size_t off) -> char* {
         char* base = nullptr;
         switch (l) {
@@ -232,26 +257,76 @@ void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
         }
         return base + off;
     };
-    for (const Step& st : plan.steps) {
-        char* src = resolve(st.src, st.src_off);
-        char* dst = resolve(st.dst, st.dst_off);
-        if (st.kind == StepKind::Tile) {
+    char* src = resolve(st.src, st.src_off);
+    char* dst = resolve(st.dst, st.dst_off);
+    if (cnt >= 0) {
+        src += chunk_offset(st, true, u0, lane, cu);
+        dst += chunk_offset(st, false, u0, lane, cu);
+    }
+    if (st.kind == StepKind::Tile) {
+        if (cnt < 0) {
             check(tile_launch(st.L, src, dst, stream), "tile kernel launch");
-        } else if (st.kind == StepKind::Blue) {
-            BluesteinArgs a = st.blue;
-            a.src = src;
-            a.dst = dst;
-            check(st.blue_post ? bluestein_post(a, stream) : bluestein_pre(a, stream), "bluestein pass launch");
-        } else if (st.kind == StepKind::Tc) {
-            check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
-                            st.L.args.tw, stream),
-                  "tensor-core kernel launch");
-        } else {
-            RealPassArgs a = st.real;
-            a.src = reinterpret_cast<const float2*>(src);
-            a.dst = reinterpret_cast<float2*>(dst);
-            check(st.kind == StepKind::RealPost ? real_post(a, stream) : real_pre(a, stream), "real pass launch");
+            return;
         }
+        check(tile_launch(chunk_tile_launch(st, cnt), src, dst, stream), "tile kernel launch");
+    } else if (st.kind == StepKind::Blue) {
+        BluesteinArgs a = st.blue;
+        a.src = src;
+        a.dst = dst;
+        check(st.blue_post ? bluestein_post(a, stream) : bluestein_pre(a, stream), "bluestein pass launch");
+    } else if (st.kind == StepKind::Tc) {
+        check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
+                        st.L.args.tw, stream),
+              "tensor-core kernel launch");
+    } else {
+        RealPassArgs a = st.real;
+        a.src = reinterpret_cast<const float2*>(src);
+        a.dst = reinterpret_cast<float2*>(dst);
+        if (cnt >= 0) a.rows = cnt * st.chunk_per;
+        check(st.kind == StepKind::RealPost ? real_post(a, stream) : real_pre(a, stream), "real pass launch");
+    }
+}
+
+}  // namespace
+
+// Steps of a chunk group run chunk by chunk: every step of the group on
+// units [u0, u0 + cu), then the next chunk.  The workspace regions of the
+// group are reused by every chunk, so the intermediate one step writes and
+// the next reads stays in L2 and the chain costs about one HBM round trip
+// of its input and output instead of one per step.
+void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws) {
+    cudaStream_t stream = static_cast<cudaStream_t>(plan.stream);
+    for (size_t i = 0; i < plan.steps.size();) {
+        const int gi = plan.steps[i].chunk_group;
+        if (gi >= 0) {
+            const ChunkGroup& g = plan.chunk_groups[gi];
+            const long long cu = chunk_units(g);
+            if (cu < g.units) {
+                // lane 0 is the plan's stream; lane 1 forks from it and joins
+                // it again after the group
+                const bool two = plan.lanes != nullptr && chunk_lanes() == 2;
+                cudaStream_t side = two ? plan.lanes->side : nullptr;
+                if (two) {
+                    check(cudaEventRecord(plan.lanes->fork, stream), "cudaEventRecord");
+                    check(cudaStreamWaitEvent(side, plan.lanes->fork, 0), "cudaStreamWaitEvent");
+                }
+                int k = 0;
+                for (long long u0 = 0; u0 < g.units; u0 += cu, ++k) {
+                    const long long cnt = std::min(cu, g.units - u0);
+                    const int lane = two ? (k & 1) : 0;
+                    for (size_t j = g.first; j < g.last; ++j)
+                        launch_one(plan.steps[j], lane ? side : stream, in, out, ws, u0, cnt, lane, cu);
+                }
+                if (two) {
+                    check(cudaEventRecord(plan.lanes->join, side), "cudaEventRecord");
+                    check(cudaStreamWaitEvent(stream, plan.lanes->join, 0), "cudaStreamWaitEvent");
+                }
+                i = g.last;
+                continue;
+            }
+        }
+        launch_one(plan.steps[i], stream, in, out, ws, 0, -1);
+        ++i;
     }
 }
 

@@ -172,7 +172,7 @@ JitCfg cfg_of(const SkEntry& e) {
     c.radices = e.radices;
     c.LD = e.LD;
     c.smem = e.smem;
-    c.twb = e.twb ? 1 : 0;
+    c.twb = e.flags;
     return c;
 }
 
@@ -262,8 +262,8 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     c.radices = jit_radices(n);
     // Tuning overrides (sweeps; unset in normal use): SIP_FFT_JIT_RADICES
     // ("25,15,8", must multiply to n), SIP_FFT_JIT_P, SIP_FFT_JIT_T,
-    // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES, SIP_FFT_JIT_TWB (0: full twiddle
-    // table instead of the basis table).
+    // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES, SIP_FFT_JIT_TWB (the SK_TW_* bits
+    // of sk_kernel.cuh: basis table, twiddles in shared memory, mirrored pairs).
     if (const char* rs = std::getenv("SIP_FFT_JIT_RADICES")) {
         std::vector<int> r;
         long long prod = 1;
@@ -302,16 +302,24 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     c.T = T;
     const int r0 = c.radices[0];
     c.LD = sk_pitch(n, r0);
+    // twiddle options (SK_TW_* bits; SIP_FFT_JIT_TWB overrides them): mirrored
+    // butterfly pairs apply to real half-length tiles of two or more passes
+    c.twb = env_int("SIP_FFT_JIT_TWB", c.twb);
+    if (c.twb < 0 || c.twb > 15) return false;
+    if ((c.twb & SK_MIRROR_PAIR) && (!real_op || c.radices.size() < 2)) c.twb &= ~SK_MIRROR_PAIR;
+    if ((c.twb & SK_SPLIT_PASS0) && (c.radices.size() < 2 || op == OP_PC)) c.twb &= ~SK_SPLIT_PASS0;
+    const long long tws =
+        (long long)sk_tws_values(op, n, c.radices.data(), (int)c.radices.size(), c.twb) * 8;
     const long long buf = (long long)sk_buffer_values(op, c.P, n, r0) * 8;
-    if (2 * buf <= kMaxTileSmem) c.stages = 2;
-    else if (buf <= kMaxTileSmem) c.stages = 1;
+    if (2 * buf + tws <= kMaxTileSmem) c.stages = 2;
+    else if (buf + tws <= kMaxTileSmem) c.stages = 1;
     else return false;
     if (env_int("SIP_FFT_JIT_STAGES", 0) == 1) c.stages = 1;
-    c.smem = (int)(c.stages * buf);
+    if (c.stages != 2) c.twb &= ~SK_SPLIT_PASS0;  // a split pass 0 uses the second buffer as its work layout
+    c.smem = (int)(c.stages * buf + tws);
     const int smem_ctas = std::max<int>(1, (228 * 1024) / (c.smem + 1024));
     c.minb = std::max(1, std::min(65536 / (T * 128), smem_ctas));
     if (env_int("SIP_FFT_JIT_MINB", 0) > 0) c.minb = env_int("SIP_FFT_JIT_MINB", 0);
-    if (env_int("SIP_FFT_JIT_TWB", 1) == 0) c.twb = 0;
     *out = c;
     return true;
 }
@@ -550,7 +558,8 @@ const SkEntry* entry_of(const JitCfg& c) {
     e.mode = c.mode;
     e.sign = c.sign;
     e.tw4 = c.tw4;
-    e.twb = c.twb != 0;
+    e.twb = (c.twb & SK_TW_BASIS) != 0;
+    e.flags = c.twb;
     e.stages = c.stages;
     e.radices = c.radices;
     e.LD = c.LD;
@@ -683,10 +692,32 @@ void after_fork_child() {
     g_forked_child = true;
 }
 
+// One small compilation on the calling thread before the first background
+// job.  The compiler sets up much of its internal state (and registers the
+// exit-time teardown of it) on its first compilation; doing that here, ahead
+// of the drain handler's registration, puts the drain before that teardown
+// at exit, so that a compilation still running when the process exits does
+// not meet a compiler whose state is being destroyed (a crash observed when a
+// process exited a fraction of a second after starting background jobs).
+void nvrtc_warmup() {
+    const Nvrtc& api = nvrtc();
+    if (!api.ok) return;
+    nvrtcProgram prog = nullptr;
+    const char* src = "extern \"C\" __global__ void sip_fft_warmup(float* p) { p[threadIdx.x] *= 2.0f; }\n";
+    if (api.create(&prog, src, "sip_fft_warmup.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) return;
+    std::vector<const char*> opts(std::begin(kOptions), std::end(kOptions));
+    opts.push_back("--ptxas-options=-v");
+    (void)api.compile(prog, (int)opts.size(), opts.data());
+    size_t cs = 0;
+    (void)api.cubin_size(prog, &cs);
+    api.destroy(&prog);
+}
+
 JitWorkers& workers() {
     static JitWorkers* w = [] {
         JitWorkers* p = new JitWorkers;
         pthread_atfork(&before_fork, &after_fork_parent, &after_fork_child);
+        nvrtc_warmup();
         register_drain();
         return p;
     }();

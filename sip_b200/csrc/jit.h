@@ -31,7 +31,7 @@ struct JitCfg {
     int n = 0, P = 1, T = 32, stages = 2, minb = 1;
     std::vector<int> radices;
     int LD = 0, smem = 0;
-    int twb = 1;  // pass twiddles: 1 basis table, 0 full Stockham table (SkCfg TWB)
+    int twb = 1;  // SkCfg TWB bits: SK_TW_BASIS (else the full Stockham table), SK_TW_SMEM, SK_MIRROR_PAIR
 };
 
 // Host-side configuration for at most `values` values per thread and pass

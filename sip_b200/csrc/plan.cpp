@@ -10,6 +10,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -582,6 +583,8 @@ void add_shifted_c2c(FftPlan& plan) {
                                "c2c axis 1 n=" + std::to_string(Y));
     rows.src = Loc::In;
     rows.dst = Loc::Ws;
+    rows.chunk_dim = 1;
+    rows.chunk_per = X;
     plan.steps.push_back(rows);
     AxisIO c;
     c.inner = Y;
@@ -596,6 +599,8 @@ void add_shifted_c2c(FftPlan& plan) {
                                "c2c axis 0 n=" + std::to_string(X));
     cols.src = Loc::Ws;
     cols.dst = Loc::Out;
+    cols.chunk_dim = 2;
+    cols.chunk_per = 1;
     set_out_shift(cols, plan, X, Y);
     plan.steps.push_back(cols);
     plan.workspace_need = (size_t)(b * X * Y * 8);
@@ -773,6 +778,7 @@ void add_real_rows(FftPlan& plan, bool r2c, long long n, long long rows, Loc src
         st.tw2_kind = 1;
         st.tw2_n = n;
         st.tw2_count = m + 1;
+        st.batch_dim = 1;
         st.src = src;
         st.dst = dst;
         plan.steps.push_back(st);
@@ -832,6 +838,7 @@ Step mirrored_step(const SkEntry* e, int n, int n_other, long long rows, const A
     st.tw2_n = tw_n;
     st.tw2_count = (1LL << shift) + (tw_n + (1LL << shift) - 1) / (1LL << shift);
     L.grid = a.ntiles;
+    st.batch_dim = 2;
     st.what = what + " [sk mirrored P=" + std::to_string(e->P) + "]";
     return st;
 }
@@ -990,7 +997,202 @@ bool apply_tune_cache(FftPlan& plan) {
     return hit;
 }
 
+namespace {
+
+std::atomic<long long> g_chunk_override{-1};
+
+long long chunk_target_bytes() {
+    const long long o = g_chunk_override.load();
+    if (o >= 0) return o;
+    static const long long target = [] {
+        const char* e = std::getenv("SIP_FFT_L2_CHUNK_MB");
+        if (e == nullptr || *e == '\0') return kL2ChunkBytes;
+        const long long mb = std::atoll(e);
+        return mb <= 0 ? 0LL : mb << 20;
+    }();
+    return target;
+}
+
+// Operand bytes one chunk unit spans on the input and output side of a step.
+void chunk_slices(const Step& st, long long* in_b, long long* out_b) {
+    if (st.kind == StepKind::Tile) {
+        const TileArgs& a = st.L.args;
+        *in_b = (st.chunk_dim == 2 ? a.in_odist : a.in_idist) * st.chunk_per * 8;
+        *out_b = (st.chunk_dim == 2 ? a.out_odist : a.out_idist) * st.chunk_per * 8;
+    } else {
+        *in_b = st.real.in_pitch * 8 * st.chunk_per;
+        *out_b = st.real.out_pitch * 8 * st.chunk_per;
+    }
+}
+
+// Makes steps [first, last) one chunk group of `units` units when every
+// step can run on a slice of the units: tile steps with a chunk dimension
+// (not the two-rows-per-transform real ops) and the real pre/post passes.
+// Input and output operands move by one slice per unit; workspace regions
+// are reused by every chunk (a group holds every step that writes or reads
+// them, so each chunk's intermediate is its own).
+bool make_chunk_group(FftPlan& plan, size_t first, size_t last, long long units) {
+    if (last - first < 2 || units < 2) return false;
+    ChunkGroup g;
+    g.first = first;
+    g.last = last;
+    g.units = units;
+    for (size_t i = first; i < last; ++i) {
+        const Step& st = plan.steps[i];
+        if (st.chunk_group >= 0) return false;
+        if (st.kind == StepKind::Tile) {
+            if (st.chunk_dim != 1 && st.chunk_dim != 2) return false;
+            if (st.L.op == OP_R2C_PAIR || st.L.op == OP_C2R_PAIR) return false;
+        } else if (st.kind != StepKind::RealPre && st.kind != StepKind::RealPost) {
+            return false;
+        }
+        long long ib = 0, ob = 0;
+        chunk_slices(st, &ib, &ob);
+        g.unit_bytes = std::max(g.unit_bytes, std::max(ib, ob));
+    }
+    for (size_t i = first; i < last; ++i) {
+        Step& st = plan.steps[i];
+        long long ib = 0, ob = 0;
+        chunk_slices(st, &ib, &ob);
+        st.chunk_group = (int)plan.chunk_groups.size();
+        st.chunk_src = ib;
+        st.chunk_dst = ob;
+    }
+    plan.chunk_groups.push_back(g);
+    return true;
+}
+
+// Chunk groups of a built plan.  1-D plans (and pulse plans): every step
+// carries the batch rows, so the whole chain runs row chunk by row chunk.
+// Multi-D plans: whole batch items per chunk when an item fits the chunk
+// size; otherwise, for 3-D, slabs of the outermost axis through the last-axis
+// pass and the pass along the middle axis (the outermost-axis pass then runs
+// over the whole volume).  Plans with other step kinds run unchunked.
+void form_chunk_groups(FftPlan& plan) {
+    plan.chunk_groups.clear();
+    for (Step& st : plan.steps) st.chunk_group = -1;
+    const size_t ns = plan.steps.size();
+    if (ns < 2) return;
+    if (plan.sizes.size() == 1 || plan.pulse) {
+        for (Step& st : plan.steps)
+            if (st.kind == StepKind::Tile) {
+                st.chunk_dim = st.batch_dim;
+                st.chunk_per = 1;
+            }
+        make_chunk_group(plan, 0, ns, plan.batch);
+        return;
+    }
+    // Multi-D chunks only on request (SIP_FFT_L2_CHUNK_MB or the test hook):
+    // measured slower than the unchunked axis passes on B200 (2048^2 x 8:
+    // 0.34 ms unchunked, 0.38-0.40 ms in chunks of one or two items).
+    const char* req = std::getenv("SIP_FFT_L2_CHUNK_MB");
+    if (g_chunk_override.load() < 0 && (req == nullptr || *req == '\0')) return;
+    long long item = 8;
+    for (int64_t s : plan.sizes) item *= s;
+    const long long target = chunk_target_bytes();
+    if (target > 0 && item <= target) {
+        make_chunk_group(plan, 0, ns, plan.batch);
+        return;
+    }
+    if (plan.sizes.size() == 3 && ns == 3 && plan.type != ASCEND_FFT_C2R) {
+        const long long X = plan.sizes[0];
+        Step& s0 = plan.steps[0];
+        Step& s1 = plan.steps[1];
+        if (s0.chunk_dim != 1 || s1.chunk_dim != 2 || s0.chunk_per % X != 0 || s1.chunk_per % X != 0) return;
+        const long long p0 = s0.chunk_per, p1 = s1.chunk_per;
+        s0.chunk_per /= X;
+        s1.chunk_per /= X;
+        if (!make_chunk_group(plan, 0, 2, plan.batch * X)) {
+            s0.chunk_per = p0;
+            s1.chunk_per = p1;
+        }
+    }
+}
+
+void build_steps_inner(FftPlan& plan);
+
+}  // namespace
+
+void set_l2_chunk_bytes(long long bytes) { g_chunk_override.store(bytes < 0 ? -1 : bytes); }
+
+int chunk_lanes() {
+    static const int v = [] {
+        const char* e = std::getenv("SIP_FFT_L2_CHUNK_LANES");
+        return (e != nullptr && std::atoi(e) == 1) ? 1 : 2;
+    }();
+    return v;
+}
+
+long long chunk_offset(const Step& st, bool src, long long u0, int lane, long long cu) {
+    const Loc l = src ? st.src : st.dst;
+    const long long slice = src ? st.chunk_src : st.chunk_dst;
+    return l == Loc::Ws ? (long long)lane * cu * slice : u0 * slice;
+}
+
+// Smallest chunk unit that is chunked: on B200, running the passes chunk by
+// chunk (one launch per step and chunk) costs more in launch gaps and
+// partial waves than the L2 reuse saves for units of a few MB (2^20-point
+// real rows, 65536-point rows, 2048^2 items: 1.2-1.7x slower), and pays for
+// transforms of 2^21 points and more, whose strided column pass is slow
+// from HBM (c2c 2^21 x 64: 4.1 ms unchunked, 1.8 ms in chunks of two rows).
+// SIP_FFT_L2_CHUNK_MIN_MB overrides it (measurements).
+long long chunk_min_unit_bytes() {
+    if (g_chunk_override.load() >= 0) return 0;  // the test hook chunks every group
+    static const long long v = [] {
+        const char* e = std::getenv("SIP_FFT_L2_CHUNK_MIN_MB");
+        return (e != nullptr && *e != '\0') ? std::max(0LL, (long long)std::atoll(e)) << 20 : kL2ChunkMinUnit;
+    }();
+    return v;
+}
+
+long long chunk_units(const ChunkGroup& g) {
+    const long long target = chunk_target_bytes();
+    if (target <= 0 || g.unit_bytes <= 0 || g.unit_bytes < chunk_min_unit_bytes()) return g.units;
+    return std::max(1LL, std::min(g.units, target / g.unit_bytes));
+}
+
+long long exec_launches(const FftPlan& plan) {
+    long long n = 0;
+    for (size_t i = 0; i < plan.steps.size();) {
+        const int gi = plan.steps[i].chunk_group;
+        if (gi >= 0) {
+            const ChunkGroup& g = plan.chunk_groups[gi];
+            const long long cu = chunk_units(g);
+            n += (long long)(g.last - g.first) * ((g.units + cu - 1) / cu);
+            i = g.last;
+        } else {
+            ++n;
+            ++i;
+        }
+    }
+    return n;
+}
+
+TileLaunch chunk_tile_launch(const Step& st, long long cnt) {
+    TileLaunch L = st.L;
+    TileArgs& a = L.args;
+    const long long n = cnt * st.chunk_per;
+    if (st.chunk_dim == 1) {
+        const long long outer = st.L.args.ntiles / st.L.args.tiles_per_outer;
+        a.inner = (int)n;
+        a.tiles_per_outer = (int)((n + a.P - 1) / a.P);
+        a.div_tpo = make_fastdiv((uint32_t)a.tiles_per_outer);
+        a.ntiles = (int)(a.tiles_per_outer * outer);
+    } else {
+        a.ntiles = (int)(a.tiles_per_outer * n);
+    }
+    L.grid = st.max_grid > 0 ? std::min(a.ntiles, st.max_grid) : a.ntiles;
+    return L;
+}
+
 void build_steps(FftPlan& plan) {
+    build_steps_inner(plan);
+    form_chunk_groups(plan);
+}
+
+namespace {
+
+void build_steps_inner(FftPlan& plan) {
     g_compute_mode = plan.compute_mode;
     g_hint_p = plan.hint_p;
     g_hint_e = plan.hint_e;
@@ -1077,7 +1279,16 @@ void build_steps(FftPlan& plan) {
                                  "c2c axis " + std::to_string(ax) + " n=" + std::to_string(n));
         st.src = src;
         st.dst = dst;
+        st.chunk_dim = 2;  // outer index: the batch item, then the axes before ax
+        st.chunk_per = outer / b;
         plan.steps.push_back(st);
+    };
+    // the contiguous last-axis pass: rows / b rows per batch item
+    auto rows_chunks = [&]() {
+        Step& st = plan.steps.back();
+        if (st.L.op == OP_R2C_PAIR || st.L.op == OP_C2R_PAIR) return;  // two rows per transform
+        st.chunk_dim = 1;
+        st.chunk_per = rows / b;
     };
     if (c2c) {
         AxisIO io;
@@ -1089,17 +1300,22 @@ void build_steps(FftPlan& plan) {
         st.src = Loc::In;
         st.dst = Loc::Out;
         plan.steps.push_back(st);
+        rows_chunks();
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else if (r2c) {
         add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
+        rows_chunks();
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else {
         column_pass(nd - 2, Loc::In, Loc::Ws);
         for (int ax = nd - 3; ax >= 0; --ax) column_pass(ax, Loc::Ws, Loc::Ws);
         add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
+        rows_chunks();
         plan.workspace_need = (size_t)(rows * lastc * 8);
     }
 }
+
+}  // namespace
 
 std::string describe(const FftPlan& plan) {
     static const char* locs[] = {"in", "out", "ws"};
@@ -1107,12 +1323,19 @@ std::string describe(const FftPlan& plan) {
     os << "{\"type\":" << (int)plan.type << ",\"forward\":" << (plan.forward() ? "true" : "false")
        << ",\"batch\":" << plan.batch << ",\"sizes\":[";
     for (size_t i = 0; i < plan.sizes.size(); ++i) os << (i ? "," : "") << plan.sizes[i];
-    os << "],\"workspace\":" << plan.workspace_need << ",\"steps\":[";
+    os << "],\"workspace\":" << plan.workspace_need << ",\"launches\":" << exec_launches(plan)
+       << ",\"chunk_groups\":[";
+    for (size_t i = 0; i < plan.chunk_groups.size(); ++i) {
+        const ChunkGroup& g = plan.chunk_groups[i];
+        os << (i ? "," : "") << "{\"first\":" << g.first << ",\"last\":" << g.last << ",\"units\":" << g.units
+           << ",\"unit_bytes\":" << g.unit_bytes << ",\"chunk_units\":" << chunk_units(g) << "}";
+    }
+    os << "],\"steps\":[";
     for (size_t i = 0; i < plan.steps.size(); ++i) {
         const Step& st = plan.steps[i];
         os << (i ? "," : "") << "{\"what\":\"" << st.what << "\",\"kind\":" << (int)st.kind << ",\"src\":\""
            << locs[(int)st.src] << "\",\"dst\":\"" << locs[(int)st.dst] << "\",\"src_off\":" << st.src_off
-           << ",\"dst_off\":" << st.dst_off;
+           << ",\"dst_off\":" << st.dst_off << ",\"chunk_group\":" << st.chunk_group;
         if (st.kind == StepKind::Tile || st.kind == StepKind::Tc) {
             const TileArgs& a = st.L.args;
             os << ",\"op\":" << st.L.op << ",\"sign\":" << st.L.sign << ",\"e\":" << st.L.e << ",\"n\":" << a.N

@@ -73,6 +73,37 @@ struct Step {
     BufPtr tc_bmat;
     BufPtr plan_dev, tw, tw2;
     std::string what;                 // human-readable description
+    // L2-resident chunks (launch_steps): the steps of one chunk group run
+    // back to back on a slice of `units` chunk units at a time, so that what
+    // one step writes for the next is still in L2.  chunk_dim is the tile
+    // index that carries the units (1 inner, 2 outer; RealPre/RealPost steps
+    // use their rows), chunk_per its count per unit, chunk_src / chunk_dst the
+    // bytes one unit spans in the source / destination operand.  Input and
+    // output operands move by one slice per unit; a workspace operand does
+    // not: every chunk of a lane reuses the same region (lane l at l chunks'
+    // worth of slices), which stays in L2.
+    int chunk_group = -1;
+    int chunk_dim = 0;
+    long long chunk_per = 1;
+    long long chunk_src = 0, chunk_dst = 0;
+    int max_grid = 0;  // resident CTAs of a persistent (sk) kernel; 0: one CTA per tile
+};
+
+// The second stream and the fork / join events of a plan's chunk lanes.
+struct ChunkLanes {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~ChunkLanes();
+};
+
+// Steps [first, last) of a plan that run chunk by chunk; `units` chunk units
+// in all, `unit_bytes` the largest operand slice of one unit.  Consecutive
+// chunks alternate between the plan's stream and a second stream (two
+// lanes), so that one chunk's passes overlap the next one's.
+struct ChunkGroup {
+    size_t first = 0, last = 0;
+    long long units = 0;
+    long long unit_bytes = 0;
 };
 
 struct FftPlan {
@@ -107,7 +138,15 @@ struct FftPlan {
     void* workspace = nullptr;
     size_t workspace_recorded = 0;  // value recorded by GetWorkspaceSize
     size_t workspace_need = 0;
+    // Device address of the static scratch array of sipFftExecC2CNoAlloc
+    // (noalloc.cu), resolved while the plan is prepared on its device for
+    // FP32 C2C plans whose workspace fits the array; null otherwise.
+    void* noalloc_scratch = nullptr;
     std::vector<Step> steps;
+    std::vector<ChunkGroup> chunk_groups;
+    // Second stream and fork / join events of the two chunk lanes (made at
+    // device preparation when the plan has chunk groups).
+    std::shared_ptr<ChunkLanes> lanes;
 
     bool forward() const { return direction == AsdSip::ASCEND_FFT_FORWARD; }
     int64_t elements() const;  // batch * prod(sizes)
@@ -158,8 +197,31 @@ int batch_last_launches(const Batch* b);
 // float planes.
 void launch_separated(const FftPlan& plan, const float* in_re, const float* in_im, float* out_re, float* out_im);
 
-// Launches every step on the plan's stream.
+// Launches every step on the plan's stream (chunk groups chunk by chunk).
 void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws);
+
+// Chunk units per chunk of a group for the current L2 chunk size
+// (SIP_FFT_L2_CHUNK_MB, default kL2ChunkBytes; 0 turns chunking off); the
+// group's `units` when it runs as one launch per step.
+long long chunk_units(const ChunkGroup& g);
+constexpr long long kL2ChunkBytes = 32LL << 20;
+// Units smaller than this run unchunked (plan.cpp chunk_min_unit_bytes).
+constexpr long long kL2ChunkMinUnit = 16LL << 20;
+// Overrides the chunk size for plans made and execs run afterwards (0 turns
+// chunking off; a negative value restores the default).
+void set_l2_chunk_bytes(long long bytes);
+// Chunk lanes (1 or 2; SIP_FFT_L2_CHUNK_LANES, default 2).
+int chunk_lanes();
+// Byte offset of a step operand for chunk units [u0, ...) on lane `lane`
+// with `cu` units per chunk.
+long long chunk_offset(const Step& st, bool src, long long u0, int lane, long long cu);
+
+// Kernel launches one exec of the plan makes (chunking included).
+long long exec_launches(const FftPlan& plan);
+
+// The launch of a tile step restricted to `cnt` chunk units of its group
+// (tile counts and the persistent grid recomputed).
+TileLaunch chunk_tile_launch(const Step& st, long long cnt);
 
 // JSON description of the steps (tests, ASDSIP_FFT_PLAN_TRACE).
 std::string describe(const FftPlan& plan);

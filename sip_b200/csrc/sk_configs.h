@@ -1,8 +1,10 @@
 // Compiled size-specialized tile kernels:
 //   X(shard, N, P, T, OP, MODE, SIGN, TW4, STAGES, MINB, TWB, radices...)
 // MINB is the CTAs-per-SM register target (__launch_bounds__), chosen so
-// that the kernel does not spill.  TWB selects basis (1) or full (0) pass
-// twiddles (sk_kernel.cuh SkCfg::TWB).
+// that the kernel does not spill.  TWB holds the sk_kernel.cuh SK_* bits:
+// 1 basis (else full) pass twiddles, 2 twiddles staged in shared memory,
+// 4 mirrored butterfly pairs in the real tiles' last (R2C) or first (C2R)
+// pass, 8 pass 0 from the staging buffer into a separate work buffer.
 // Every other length runs on the generic tile kernel.  The shard index
 // spreads the instantiations over parallel compile units.  Several entries
 // for the same (N, OP, MODE, SIGN, TW4) are variants of the tile shape or
@@ -12,8 +14,8 @@
 
 #define SIP_SK_CONFIGS(X)                                                     \
     /* 1D / last-axis C2C rows */                                             \
-    X(0, 4096, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 16)              \
-    X(1, 4096, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 16)               \
+    X(0, 4096, 1, 128, OP_C2C, SK_ROWS, -1, false, 2, 3, 9, 16, 16, 16)              \
+    X(1, 4096, 1, 128, OP_C2C, SK_ROWS, 1, false, 2, 3, 9, 16, 16, 16)               \
     X(2, 2048, 2, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 8)               \
     X(3, 2048, 2, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 8)                \
     X(4, 1024, 4, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 4)               \
@@ -37,23 +39,28 @@
     X(3, 512, 16, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 1, 16, 32)                    \
     X(4, 1024, 8, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 32, 32)                \
     X(5, 1024, 8, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 32, 32)                 \
-    /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000); the   \
-       first entry of each is the default, the second a hint variant */     \
-    X(0, 500, 4, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 1, 25, 20)              \
-    X(6, 500, 8, 200, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 20)              \
-    X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 1, 25, 20)               \
-    X(7, 500, 8, 200, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 20)               \
-    X(2, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 1, 25, 15, 8)          \
-    X(0, 3000, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 1, 25, 15, 8)          \
-    X(1, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 15, 8)           \
-    X(3, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 1, 25, 15, 8)           \
+    /* real rows: R2C / C2R of N = 1000, 6000 (half length 500, 3000).  The  \
+       defaults split pass 0 (TWB 8: staging buffer -> work buffer, next tile \
+       staged after it), keep the twiddles in shared memory (2) and, for     \
+       R2C, run the last pass as mirrored butterfly pairs with the post-     \
+       process fused (4); small CTAs (2-4 warps) leave more of them per SM.  \
+       The second entry of a length is a hint variant. */                    \
+    X(0, 500, 2, 64, OP_R2C_HALF, SK_ROWS, -1, false, 2, 8, 15, 25, 5, 4)            \
+    X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 5, 10, 10)           \
+    X(2, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 15, 25, 15, 8)         \
+    X(3, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 9, 25, 8, 15)           \
+    X(4, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 7, 15, 25, 8)          \
+    X(5, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 8, 15)           \
     /* real rows of N = 2048, 4096, 8192 (half lengths 1024, 2048, 4096) */  \
-    X(4, 1024, 4, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 4)          \
-    X(5, 1024, 4, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 4)           \
-    X(6, 2048, 2, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 8)          \
-    X(7, 2048, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 8)           \
-    X(0, 4096, 1, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 16)         \
-    X(1, 4096, 1, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 16)          \
+    X(6, 1024, 4, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 15, 16, 16, 4)         \
+    X(7, 1024, 4, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 9, 4, 16, 16)           \
+    X(0, 2048, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 15, 16, 16, 8)         \
+    X(1, 2048, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 8, 16, 16)          \
+    X(2, 4096, 1, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 15, 16, 32, 8)         \
+    X(3, 4096, 1, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 15, 16, 16, 16)         \
+    X(4, 1024, 4, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 3, 7, 16, 16, 4)          \
+    X(5, 2048, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 7, 16, 16, 8)          \
+    X(6, 4096, 1, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 7, 16, 32, 8)          \
     /* 2D 500 x 50 (the reference's MRI example shape): rows of 50, columns \
        of 500 over the 50-wide slices */                                     \
     X(2, 50, 16, 128, OP_C2C, SK_ROWS, -1, false, 2, 4, 1, 5, 10)                    \
@@ -62,11 +69,17 @@
     X(5, 500, 10, 256, OP_C2C, SK_COLS, 1, false, 2, 2, 1, 25, 20)                   \
     /* odd real length 2187 = 3^7, two rows per complex FFT (the R2C tile  \
        shape from a run-time compiled sweep: 4 % faster than 2 x 192) */     \
-    X(2, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 1, 27, 9, 9)           \
-    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
+    X(7, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 15, 27, 9, 9)          \
+    X(0, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 9, 27, 9, 9)            \
+    X(1, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 1, 27, 9, 9)           \
+    X(2, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
     /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A        \
        (planner hint) */                                                     \
     X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)            \
-    X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)
+    X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)                \
+    /* the C2R form with mirrored pairs in its split pass 0: a hint variant  \
+       (slower than the plain split pass for N = 6000) */                   \
+    X(6, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 15, 25, 8)          \
+    X(7, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 15, 9, 9, 27)
 
 #define SIP_SK_SHARDS 8

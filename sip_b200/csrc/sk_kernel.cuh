@@ -36,6 +36,48 @@ SIP_HD constexpr int sk_index(int n, int r0) { return r0 % 2 == 0 ? n + n / sk_p
 SIP_HD constexpr int sk_pitch(int n, int r0) {
     return ((sk_index(n - 1, r0) + 1) & 1) ? sk_index(n - 1, r0) + 1 : sk_index(n - 1, r0) + 2;
 }
+// Bits of a configuration's TWB parameter (SkCfg):
+//   SK_TW_BASIS     pass twiddles from the basis table (fewer loads, one
+//                   product more) instead of the full Stockham table;
+//   SK_TW_SMEM      the pass twiddle table and the real pre/post-process
+//                   twiddles are copied to shared memory once per
+//                   persistent CTA and read from there;
+//   SK_MIRROR_PAIR  real tiles: the last pass of an R2C (first pass of a
+//                   C2R) gives each thread butterfly u and its mirror
+//                   NR - u, so that the post-process (pre-process) runs on
+//                   registers (sk_pair_last_r2c, SkPairFirstC2R);
+//   SK_SPLIT_PASS0  pass 0 reads the staging buffer and writes the work
+//                   layout into the other buffer, one butterfly (pair) at a
+//                   time instead of all of them across a barrier; the next
+//                   tile is staged after pass 0 (overlapping the later
+//                   passes) instead of before it.
+enum : int { SK_TW_BASIS = 1, SK_TW_SMEM = 2, SK_MIRROR_PAIR = 4, SK_SPLIT_PASS0 = 8 };
+
+SIP_HD constexpr int sk_twcount(int r, bool basis) { return basis ? basis_count(r) : r - 1; }
+// Entries per table row of pass p in shared memory: all L values k of the
+// span, or k <= L/2 for the mirrored last pass of an R2C tile (its butterfly
+// pairs read only those).
+SIP_HD constexpr int sk_tws_stride(int op, int flags, int p, int np, int L) {
+    return ((flags & SK_MIRROR_PAIR) && (op == OP_R2C_HALF || op == OP_R2C_PAIR) && p == np - 1) ? L / 2 + 1 : L;
+}
+// Real pre/post-process twiddles W_{2M}^k staged in shared memory (k < count).
+SIP_HD constexpr int sk_tw2s(int op, int n, int r0, int rlast, int flags) {
+    return !(flags & SK_TW_SMEM) ? 0
+         : op == OP_R2C_HALF ? ((flags & SK_MIRROR_PAIR) ? n / rlast / 2 + 1 : n / 2 + 1)
+         : op == OP_C2R_HALF ? ((flags & SK_MIRROR_PAIR) ? n / r0 / 2 + 1 : n)
+         : 0;
+}
+// Complex values of shared memory the staged twiddles take (even count).
+SIP_HD constexpr int sk_tws_values(int op, int n, const int* rs, int np, int flags) {
+    int total = 0, L = 1;
+    for (int p = 0; p < np; ++p) {
+        if (L > 1) total += sk_twcount(rs[p], (flags & SK_TW_BASIS) != 0) * sk_tws_stride(op, flags, p, np, L);
+        L *= rs[p];
+    }
+    total += sk_tw2s(op, n, rs[0], rs[np - 1], flags);
+    return (flags & SK_TW_SMEM) ? (total + 1) / 2 * 2 : 0;
+}
+
 // Staged input values (complex64 units) per tile.
 SIP_HD constexpr int sk_stage_values(int op, int p, int n) {
     return op == OP_C2R_HALF ? p * (n + 1)
@@ -70,10 +112,17 @@ struct SkCfg {
         for (int i = 0; i < p; ++i) l *= radix(i);
         return l;
     }
-    // Pass twiddles: TWB = 1 reads the basis table (fft_core.cuh
-    // basis_split: fewer loads, one extra product), TWB = 0 the full
+    // Pass twiddles: SK_TW_BASIS reads the basis table (fft_core.cuh
+    // basis_split: fewer loads, one extra product), else the full
     // Stockham table (one load per twiddle, fewer instructions).
-    static constexpr bool TWB = TWB_ != 0;
+    static constexpr int FLAGS = TWB_;
+    static constexpr bool TWB = (TWB_ & SK_TW_BASIS) != 0;
+    static constexpr bool TWS = (TWB_ & SK_TW_SMEM) != 0;
+    static constexpr bool MPAIR = (TWB_ & SK_MIRROR_PAIR) != 0;
+    static constexpr bool SPLIT = (TWB_ & SK_SPLIT_PASS0) != 0;
+    // The configuration's own operation (SkView below re-labels OP for the
+    // halves of a pulse tile; the staged twiddle layout follows CFG_OP).
+    static constexpr int CFG_OP = OP_;
     static constexpr int twcount(int r) { return TWB ? basis_count(r) : r - 1; }
     static constexpr int twoff(int p) {  // offset of pass p in the twiddle table
         int off = 0;
@@ -95,7 +144,19 @@ struct SkCfg {
     static constexpr int LD = sk_pitch(N, radix(0));
     static constexpr int STAGE = sk_stage_values(OP, P, N);
     static constexpr int BUF = sk_buffer_values(OP, P, N, radix(0));
-    static constexpr int SMEM = 2 * BUF * 8;
+    // Staged twiddles (SK_TW_SMEM): per pass p with span > 1, twcount rows
+    // of tws_stride(p) entries from tws_off(p), then TW2S real twiddles.
+    static constexpr int tws_stride(int p) { return sk_tws_stride(CFG_OP, FLAGS, p, NP, span(p)); }
+    static constexpr int tws_off(int p) {
+        int off = 0;
+        for (int i = 0; i < p; ++i)
+            if (span(i) > 1) off += twcount(radix(i)) * tws_stride(i);
+        return off;
+    }
+    static constexpr int TW2_OFF = tws_off(NP);
+    static constexpr int TW2S = sk_tw2s(CFG_OP, N, radix(0), radix(NP - 1), FLAGS);
+    static constexpr int TWSM = TWS ? (TW2_OFF + TW2S + 1) / 2 * 2 : 0;
+    static constexpr int SMEM = 2 * BUF * 8 + TWSM * 8;
     // CTAs per SM the shared memory allows with two stages (228 KB per SM,
     // 1 KB reserved per CTA); used as the register-allocation target.
     static constexpr int smem_ctas(int stages) {
@@ -111,8 +172,17 @@ struct SkCfg {
     static constexpr bool WORK_IN = false;
 
     static_assert(span(NP) == N, "radices must multiply to N");
-    static_assert(OP != OP_C2C || MODE != SK_COLS || true, "");
     static_assert(!(TW4 && OP != OP_C2C && OP != OP_PC), "cross twiddles are C2C / pulse only");
+    static_assert(!MPAIR || ((OP == OP_R2C_HALF || OP == OP_C2R_HALF || OP == OP_R2C_PAIR || OP == OP_C2R_PAIR) &&
+                             MODE == SK_ROWS && NP >= 2),
+                  "mirrored butterfly pairs: real rows of two or more passes");
+    static_assert(!MPAIR || (OP != OP_R2C_HALF && OP != OP_R2C_PAIR) || SIGN < 0,
+                  "R2C tiles run the forward transform");
+    static_assert(!MPAIR || (OP != OP_C2R_HALF && OP != OP_C2R_PAIR) || SIGN > 0,
+                  "C2R tiles run the inverse transform");
+    static_assert(!SPLIT || (NP >= 2 && OP != OP_PC), "a split pass 0 needs a later pass, and no pulse tile");
+    static constexpr int rad_list[] = {Rs...};
+    static_assert(TWSM == sk_tws_values(OP_, N_, rad_list, NP, TWB_), "staged twiddle layout");
 };
 
 // A configuration seen with another operation, direction and pass-0 source:
@@ -126,6 +196,75 @@ struct SkView : K {
     static constexpr int SIGN = SIGN_;
     static constexpr bool WORK_IN = WORK_IN_;
 };
+
+// ------------------------------------------------------------ twiddles
+// Entry t (1-based row of the basis or full table) at span index k of pass
+// PASS: from shared memory (SK_TW_SMEM) or through the read-only cache.
+template <class K, int PASS>
+SIP_HD float2 sk_ptw(const TileArgs& a, const TileCtx& c, int t, int k) {
+    if constexpr (K::TWS)
+        return c.tws[K::tws_off(PASS) + (t - 1) * K::tws_stride(PASS) + k];
+    else
+        return SIP_LDG(a.tw + K::twoff(PASS) + (t - 1) * K::span(PASS) + k);
+}
+
+// Real pre/post-process twiddle W_{2M}^k (the tile's tw2 root table).
+template <class K>
+SIP_HD float2 sk_tw2(const TileArgs& a, const TileCtx& c, int k) {
+    if constexpr (K::TWS && K::TW2S > 0)
+        return c.tws[K::TW2_OFF + k];
+    else
+        return SIP_LDG(a.tw2 + k);
+}
+
+// w[r] = W_{L R}^{r k} for 1 <= r < R (forward values; w[0] is unused):
+// one table load each, or basis products W^{r_lo k} W^{a r_hi k}.
+template <class K, int PASS, int R>
+SIP_HD void sk_pass_twiddles(const TileArgs& a, const TileCtx& c, int k, float2 (&w)[R]) {
+    if constexpr (!K::TWB) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) w[r] = sk_ptw<K, PASS>(a, c, r, k);
+    } else {
+        constexpr int A = basis_split(R);
+        float2 lo[A], hi[R / A];
+        lo[0] = make_float2(1.f, 0.f);
+        hi[0] = make_float2(1.f, 0.f);
+#pragma unroll
+        for (int t = 1; t < A; ++t) lo[t] = sk_ptw<K, PASS>(a, c, t, k);
+#pragma unroll
+        for (int t = 1; t < R / A; ++t) hi[t] = sk_ptw<K, PASS>(a, c, A - 1 + t, k);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            const int rl = r % A, rh = r / A;
+            w[r] = rh == 0 ? lo[rl] : rl == 0 ? hi[rh] : c_mul(lo[rl], hi[rh]);
+        }
+    }
+}
+
+// Copies the pass twiddles of passes P0.. and the real twiddles to shared
+// memory (once per persistent CTA; a barrier follows before the first use).
+template <class K, int P0>
+SIP_HD void sk_load_tws_pass(int tid, const TileArgs& a, float2* tws) {
+    if constexpr (P0 < K::NP) {
+        if constexpr (K::span(P0) > 1) {
+            constexpr int L = K::span(P0), ST = K::tws_stride(P0);
+            constexpr int TOTAL = K::twcount(K::radix(P0)) * ST;
+            for (int i = tid; i < TOTAL; i += K::T) {
+                const int t = i / ST, k = i - t * ST;
+                tws[K::tws_off(P0) + i] = a.tw[K::twoff(P0) + t * L + k];
+            }
+        }
+        sk_load_tws_pass<K, P0 + 1>(tid, a, tws);
+    }
+}
+
+template <class K>
+SIP_HD void sk_load_tws(int tid, const TileArgs& a, float2* tws) {
+    if constexpr (K::TWS) {
+        sk_load_tws_pass<K, 1>(tid, a, tws);
+        for (int k = tid; k < K::TW2S; k += K::T) tws[K::TW2_OFF + k] = a.tw2[k];
+    }
+}
 
 // Column index of slot q of a C2R_4A tile (-1 when the slot is unused).
 template <class K>
@@ -340,7 +479,7 @@ SIP_HD float2 sk_input(const TileArgs& a, const TileCtx& c, const float2* stage,
         const float2 x = maybe_conj(row[n], cj), y = maybe_conj(row[N - n], cj);
         const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
         const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
-        const float2 od = c_mulc(d, SIP_LDG(a.tw2 + n));
+        const float2 od = c_mulc(d, sk_tw2<K>(a, c, n));
         return make_float2(e.x - od.y, e.y + od.x);
     } else {  // OP_C2R_PAIR
         constexpr int H = N / 2 + 1;
@@ -381,63 +520,53 @@ struct SkPass {
         }
     }
 
-    // Reads (pass 0: from the staged input) and transforms this thread's butterflies.
+    // Reads (pass 0: from the staged input) and transforms butterfly slot s
+    // of this thread; false when the slot has no butterfly.
+    SIP_HD static bool read_slot(int tid, int s, const TileArgs& a, const TileCtx& c, const float2* buf,
+                                 float2 (&v)[R]) {
+        const int b = tid + s * K::T;
+        if (TOTAL % K::T != 0 && b >= TOTAL) return false;
+        int q, j;
+        butterfly_index(b, q, j);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if constexpr (PASS == 0 && !K::WORK_IN)
+                v[r] = sk_input<K>(a, c, buf, q, j + r * NR);
+            else
+                v[r] = buf[q * K::LD + K::idx(j + r * NR)];
+        }
+        if constexpr (L > 1) {
+            // twiddle-major tables: consecutive k of a warp read consecutive
+            // entries
+            float2 w[R];
+            sk_pass_twiddles<K, PASS>(a, c, j % L, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = c_tw<K::SIGN>(v[r], w[r]);
+        }
+        dft<R, K::SIGN>(v);
+        return true;
+    }
+
+    // Writes butterfly slot s to the padded work layout.
+    SIP_HD static void write_slot(int tid, int s, float2* buf, const float2 (&v)[R]) {
+        const int b = tid + s * K::T;
+        if (TOTAL % K::T != 0 && b >= TOTAL) return;
+        int q, j;
+        butterfly_index(b, q, j);
+        const int o = (j / L) * L * R + j % L;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[q * K::LD + K::idx(o + r * L)] = v[r];
+    }
+
     SIP_HD static void read(int tid, const TileArgs& a, const TileCtx& c, const float2* buf, Regs& rg) {
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int b = tid + s * K::T;
-            if (TOTAL % K::T == 0 || b < TOTAL) {
-                int q, j;
-                butterfly_index(b, q, j);
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    if constexpr (PASS == 0 && !K::WORK_IN)
-                        rg.v[s][r] = sk_input<K>(a, c, buf, q, j + r * NR);
-                    else
-                        rg.v[s][r] = buf[q * K::LD + K::idx(j + r * NR)];
-                }
-                if constexpr (L > 1 && !K::TWB) {
-                    const int k = j % L;
-                    const float2* w = a.tw + K::twoff(PASS) + k;  // twiddle-major table
-#pragma unroll
-                    for (int r = 1; r < R; ++r) rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], SIP_LDG(w + (r - 1) * L));
-                } else if constexpr (L > 1) {
-                    // basis twiddles: W^{r k} = W^{r_lo k} W^{a r_hi k}
-                    constexpr int A = basis_split(R);
-                    const int k = j % L;
-                    const float2* w = a.tw + K::twoff(PASS) + k;  // twiddle-major table
-                    float2 lo[A], hi[R / A];
-                    lo[0] = make_float2(1.f, 0.f);
-                    hi[0] = make_float2(1.f, 0.f);
-#pragma unroll
-                    for (int t = 1; t < A; ++t) lo[t] = SIP_LDG(w + (t - 1) * L);
-#pragma unroll
-                    for (int t = 1; t < R / A; ++t) hi[t] = SIP_LDG(w + (A - 1 + t - 1) * L);
-#pragma unroll
-                    for (int r = 1; r < R; ++r) {
-                        const int rl = r % A, rh = r / A;
-                        const float2 t = rh == 0 ? lo[rl] : rl == 0 ? hi[rh] : c_mul(lo[rl], hi[rh]);
-                        rg.v[s][r] = c_tw<K::SIGN>(rg.v[s][r], t);
-                    }
-                }
-                dft<R, K::SIGN>(rg.v[s]);
-            }
-        }
+        for (int s = 0; s < S; ++s) read_slot(tid, s, a, c, buf, rg.v[s]);
     }
 
     // Writes to the padded work layout (all passes except a global-storing last one).
     SIP_HD static void write_smem(int tid, float2* buf, const Regs& rg) {
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int b = tid + s * K::T;
-            if (TOTAL % K::T == 0 || b < TOTAL) {
-                int q, j;
-                butterfly_index(b, q, j);
-                const int o = (j / L) * L * R + j % L;
-#pragma unroll
-                for (int r = 0; r < R; ++r) buf[q * K::LD + K::idx(o + r * L)] = rg.v[s][r];
-            }
-        }
+        for (int s = 0; s < S; ++s) write_slot(tid, s, buf, rg.v[s]);
     }
 
     // Last pass straight to global memory: element k = j + r N/R of transform q.
@@ -490,7 +619,7 @@ struct SkPass {
 
 template <class K>
 constexpr bool sk_last_to_smem() {
-    return K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR || K::OP == OP_R2C_4B || K::OP == OP_PC;
+    return ((K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR) && !K::MPAIR) || K::OP == OP_R2C_4B || K::OP == OP_PC;
 }
 
 // R2C value X[k] from Z[k] and Z[M-k] (formula of tile_io.cuh
@@ -542,7 +671,7 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
             const float2 zm = row[K::idx(k == 0 ? 0 : M - k)];
             const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
             const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
-            const float2 t = c_mul(SIP_LDG(a.tw2 + k), od);
+            const float2 t = c_mul(sk_tw2<K>(a, c, k), od);
             float2 x = c_add(ev, t);
             if (sc) x = c_scale(x, a.scale);
             out[k] = maybe_conj(x, cj);
@@ -609,6 +738,398 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
     }
 }
 
+// ------------------------------------------------ mirrored butterfly pairs
+// SK_MIRROR_PAIR for real half-length tiles of length M (the complex FFT
+// of the packed row).  In a pass of radix R with NR = M / R butterflies and
+// span NR (the last pass; the first pass reads the same index set), the
+// elements of butterfly u are u + r NR and those of butterfly NR - u are
+// their mirrors: M - (u + r NR) = (NR - u) + (R - 1 - r) NR, and for u = 0
+// the mirror of r NR is (R - r) NR in the same butterfly (u = NR / 2 is its
+// own mirror when NR is even).  One thread takes the pair (u, NR - u), u in
+// [0, NR / 2], so each R2C output pair X[k], X[M - k] (each C2R input pair)
+// meets in its registers: the post-process stores to global memory without
+// another shared-memory round trip, and the pre-process reads every bin once.
+// The mirror's pass twiddles W_M^{r (NR - u)} = W_R^r conj(W_M^{r u}) and the
+// real twiddles W_{2M}^{u + r NR} = W_{2M}^u W_{2R}^r need table entries of
+// u only, times compile-time constants.
+
+// Compile-time loop: f(SkIC<I>{}) for I in [B, E), so that the index can be a
+// template argument (the compile-time roots of tw_const).
+template <int V>
+struct SkIC {
+    static constexpr int value = V;
+};
+template <int I, int E, class F>
+SIP_HD void sk_static_for(F&& f) {
+    if constexpr (I < E) {
+        f(SkIC<I>{});
+        sk_static_for<I + 1, E>(f);
+    }
+}
+
+// Last pass of an R2C_HALF tile, post-process fused, output to global memory.
+template <class K>
+SIP_HD void sk_pair_last_r2c(int tid, const TileArgs& a, const TileCtx& c, const float2* buf) {
+    constexpr int PASS = K::NP - 1;
+    constexpr int R = K::radix(PASS);
+    constexpr int M = K::N;
+    constexpr int NR = M / R;
+    constexpr int U = NR / 2 + 1;
+    constexpr int TOTAL = K::P * U;
+    constexpr int S = (TOTAL + K::T - 1) / K::T;
+    static_assert(K::span(PASS) == NR, "the last pass spans N / R");
+    const bool cj = (a.flags & TF_CONJ_OUT) != 0;
+    const bool sc = (a.flags & TF_SCALE) != 0;
+    float2* dst = static_cast<float2*>(a.dst);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) break;
+        const int q = f / U;
+        const int u = f - q * U;
+        if (q >= c.cnt) continue;
+        const bool mirror = u != 0 && 2 * u != NR;  // NR - u is another butterfly
+        const float2* row = buf + q * K::LD;
+        float2 A[R], B[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) A[r] = row[K::idx(u + r * NR)];
+        if (mirror) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) B[r] = row[K::idx(NR - u + r * NR)];
+        }
+        if (u != 0) {
+            float2 w[R];
+            sk_pass_twiddles<K, PASS>(a, c, u, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) A[r] = c_tw<K::SIGN>(A[r], w[r]);
+            if (mirror)
+                sk_static_for<1, R>([&](auto ic) {
+                    constexpr int r = decltype(ic)::value;
+                    B[r] = tw_const<R, r, K::SIGN>(c_tw<-K::SIGN>(B[r], w[r]));
+                });
+        }
+        dft<R, K::SIGN>(A);
+        if (mirror) dft<R, K::SIGN>(B);
+        const float2 w2u = sk_tw2<K>(a, c, u);
+        float2* out = dst + c.out_base + (long long)q * a.out_idist;
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            const int k = u + r * NR;
+            const float2 z = A[r];
+            const float2 zm = mirror ? B[R - 1 - r] : (u == 0 ? A[(R - r) % R] : A[R - 1 - r]);
+            const float2 w2 = tw_const<2 * R, r, -1>(w2u);  // W_{2M}^k
+            const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            const float2 t = c_mul(w2, od);
+            float2 x = c_add(ev, t);
+            float2 y = make_float2(ev.x - t.x, t.y - ev.y);  // X[M - k]
+            if (sc) {
+                x = c_scale(x, a.scale);
+                y = c_scale(y, a.scale);
+            }
+            out[k] = maybe_conj(x, cj);
+            // X[M - k] belongs to this thread when the mirror is another
+            // butterfly; for u = 0 only X[M] (r = 0) is not stored as some X[k]
+            if (mirror || (u == 0 && r == 0)) out[M - k] = maybe_conj(y, cj);
+        });
+    }
+}
+
+// First pass of a C2R_HALF tile from the staged bins X[0..M], pre-process
+// fused: Z[n] = E + i W_{2M}^{+n} D and Z[M - n] from X[n], X[M - n].
+template <class K>
+struct SkPairFirstC2R {
+    static constexpr int R = K::radix(0);
+    static constexpr int M = K::N;
+    static constexpr int NR = M / R;
+    static constexpr int U = NR / 2 + 1;
+    static constexpr int TOTAL = K::P * U;
+    static constexpr int S = (TOTAL + K::T - 1) / K::T;
+    struct Regs {
+        float2 a[S][R], b[S][R];
+    };
+
+    // Z[n], Z[M - n] from x = X[n], y = X[M - n] and w = W_{2M}^n.
+    SIP_HD static void prep(float2 x, float2 y, float2 w, float2& zn, float2& zm) {
+        const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
+        const float2 od = c_mulc(d, w);
+        zn = make_float2(e.x - od.y, e.y + od.x);
+        zm = make_float2(e.x + od.y, od.x - e.y);
+    }
+
+    // Unit slot s of this thread: butterflies u (into A) and NR - u (into B),
+    // pre-processed and transformed; false when the slot has no unit.
+    SIP_HD static bool read_slot(int tid, int s, const TileArgs& a, const TileCtx& c, const float2* stage,
+                                 float2 (&A)[R], float2 (&B)[R]) {
+        const bool cj = (a.flags & TF_CONJ_IN) != 0;
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) return false;
+        const int q = f / U;
+        const int u = f - q * U;
+        const float2* row = stage + q * (M + 1);
+        const float2 wu = sk_tw2<K>(a, c, u);
+        {
+            if (u == 0) {
+                const float dc = row[0].x, ny = row[M].x;
+                A[0] = make_float2(0.5f * (dc + ny), 0.5f * (dc - ny));
+                sk_static_for<1, R / 2 + 1>([&](auto ic) {
+                    constexpr int r = decltype(ic)::value;
+                    const int n = r * NR;
+                    float2 zn, zm;
+                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), zn, zm);
+                    A[r] = zn;
+                    if (2 * r != R) A[R - r] = zm;
+                });
+            } else if (2 * u == NR) {
+                sk_static_for<0, (R + 1) / 2>([&](auto ic) {
+                    constexpr int r = decltype(ic)::value;
+                    const int n = u + r * NR;
+                    float2 zn, zm;
+                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), zn, zm);
+                    A[r] = zn;
+                    if (2 * r + 1 != R) A[R - 1 - r] = zm;
+                });
+            } else {
+                sk_static_for<0, R>([&](auto ic) {
+                    constexpr int r = decltype(ic)::value;
+                    const int n = u + r * NR;
+                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), A[r],
+                         B[R - 1 - r]);
+                });
+                dft<R, K::SIGN>(B);
+            }
+            dft<R, K::SIGN>(A);
+        }
+        return true;
+    }
+
+    // Pass 0 has span 1: butterfly j writes element r to j R + r.
+    SIP_HD static void write_slot(int tid, int s, float2* buf, const float2 (&A)[R], const float2 (&B)[R]) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) return;
+        const int q = f / U;
+        const int u = f - q * U;
+        float2* row = buf + q * K::LD;
+#pragma unroll
+        for (int r = 0; r < R; ++r) row[K::idx(u * R + r)] = A[r];
+        if (u != 0 && 2 * u != NR) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) row[K::idx((NR - u) * R + r)] = B[r];
+        }
+    }
+
+    SIP_HD static void read(int tid, const TileArgs& a, const TileCtx& c, const float2* stage, Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) read_slot(tid, s, a, c, stage, rg.a[s], rg.b[s]);
+    }
+
+    SIP_HD static void write_smem(int tid, float2* buf, const Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) write_slot(tid, s, buf, rg.a[s], rg.b[s]);
+    }
+};
+
+// Last pass of an R2C_PAIR tile (real rows 2q and 2q + 1 packed as one
+// complex row Z of odd length N), the bin separation fused: bin b <= (N-1)/2
+// of the two rows is (Z[b] + conj Z[N-b]) / 2 and (Z[b] - conj Z[N-b]) / 2i.
+// For each element k of butterfly u the stored bin is min(k, N - k); its
+// partner is the mirror butterfly's element R - 1 - r (u = 0: element R - r
+// of the same butterfly, which stores only k = r NR <= (N-1)/2).
+template <class K>
+SIP_HD void sk_pair_last_r2c_rows(int tid, const TileArgs& a, const TileCtx& c, const float2* buf) {
+    constexpr int PASS = K::NP - 1;
+    constexpr int R = K::radix(PASS);
+    constexpr int N = K::N;
+    constexpr int NR = N / R;
+    constexpr int U = NR / 2 + 1;
+    constexpr int TOTAL = K::P * U;
+    constexpr int S = (TOTAL + K::T - 1) / K::T;
+    static_assert(N % 2 == 1 && K::span(PASS) == NR, "odd lengths; the last pass spans N / R");
+    const bool cj = (a.flags & TF_CONJ_OUT) != 0;
+    const bool sc = (a.flags & TF_SCALE) != 0;
+    float2* dst = static_cast<float2*>(a.dst);
+    const int r0 = 2 * c.i0;
+    const int nrows = (a.rows - r0) < 2 * c.cnt ? (a.rows - r0) : 2 * c.cnt;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) break;
+        const int q = f / U;
+        const int u = f - q * U;
+        if (2 * q >= nrows) continue;
+        const bool mirror = u != 0;  // NR is odd: no butterfly is its own mirror but u = 0
+        const float2* row = buf + q * K::LD;
+        float2 A[R], B[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) A[r] = row[K::idx(u + r * NR)];
+        if (mirror) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) B[r] = row[K::idx(NR - u + r * NR)];
+            float2 w[R];
+            sk_pass_twiddles<K, PASS>(a, c, u, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) A[r] = c_tw<K::SIGN>(A[r], w[r]);
+            sk_static_for<1, R>([&](auto ic) {
+                constexpr int r = decltype(ic)::value;
+                B[r] = tw_const<R, r, K::SIGN>(c_tw<-K::SIGN>(B[r], w[r]));
+            });
+            dft<R, K::SIGN>(B);
+        }
+        dft<R, K::SIGN>(A);
+        const long long ra = r0 + 2 * q;
+        float2* outa = dst + ra * a.out_idist;
+        float2* outb = outa + a.out_idist;
+        const bool second = 2 * q + 1 < nrows;
+        auto store = [&](int b, float2 z, float2 zm) {
+            float2 xa = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            float2 xb = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            if (sc) {
+                xa = c_scale(xa, a.scale);
+                xb = c_scale(xb, a.scale);
+            }
+            outa[b] = maybe_conj(xa, cj);
+            if (second) outb[b] = maybe_conj(xb, cj);
+        };
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            if (mirror) {
+                const int k = u + r * NR;
+                if (2 * k < N) store(k, A[r], B[R - 1 - r]);
+                else store(N - k, B[R - 1 - r], A[r]);
+            } else if constexpr (2 * r * NR < N) {
+                store(r * NR, A[r], A[(R - r) % R]);
+            }
+        });
+    }
+}
+
+// First pass of a C2R_PAIR tile from the staged spectra of real rows 2q and
+// 2q + 1 (N/2 + 1 bins each): Z[n] = Xa[n] + i Xb[n] with the Hermitian
+// halves, every staged bin read once (for bin m and its mirror N - m).
+template <class K>
+struct SkPairFirstC2RRows {
+    static constexpr int R = K::radix(0);
+    static constexpr int N = K::N;
+    static constexpr int H = N / 2 + 1;
+    static constexpr int NR = N / R;
+    static constexpr int U = NR / 2 + 1;
+    static constexpr int TOTAL = K::P * U;
+    static constexpr int S = (TOTAL + K::T - 1) / K::T;
+    static_assert(N % 2 == 1, "odd lengths");
+
+    // Z[m] (lo) and Z[N - m] (hi) from bin m of both rows, m <= N/2.
+    SIP_HD static void bins(const float2* sa, const float2* sb, int m, bool fwd, float2& lo, float2& hi) {
+        float2 xa = sa[m], xb = sb[m];
+        if (m == 0) {
+            xa.y = 0.f;
+            xb.y = 0.f;
+        }
+        const float2 plain = make_float2(xa.x - xb.y, xa.y + xb.x);    // Xa + i Xb
+        const float2 mirr = make_float2(xa.x + xb.y, xb.x - xa.y);     // conj(Xa) + i conj(Xb)
+        lo = fwd ? mirr : plain;
+        hi = fwd ? plain : mirr;
+    }
+
+    SIP_HD static bool read_slot(int tid, int s, const TileArgs& a, const TileCtx& c, const float2* stage,
+                                 float2 (&A)[R], float2 (&B)[R]) {
+        const bool fwd = (a.flags & TF_CONJ_IN) != 0;
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) return false;
+        const int q = f / U;
+        const int u = f - q * U;
+        const float2* sa = stage + (2 * q) * H;
+        const float2* sb = sa + H;
+        if (u == 0) {
+            sk_static_for<0, R / 2 + 1>([&](auto ic) {
+                constexpr int r = decltype(ic)::value;
+                float2 lo, hi;
+                bins(sa, sb, r * NR, fwd, lo, hi);
+                A[r] = lo;
+                if (r != 0) A[R - r] = hi;
+            });
+        } else {
+            sk_static_for<0, R>([&](auto ic) {
+                constexpr int r = decltype(ic)::value;
+                const int n = u + r * NR;
+                float2 lo, hi;
+                if (2 * n < N) {
+                    bins(sa, sb, n, fwd, lo, hi);
+                    A[r] = lo;
+                    B[R - 1 - r] = hi;
+                } else {
+                    bins(sa, sb, N - n, fwd, lo, hi);
+                    A[r] = hi;
+                    B[R - 1 - r] = lo;
+                }
+            });
+            dft<R, K::SIGN>(B);
+        }
+        dft<R, K::SIGN>(A);
+        return true;
+    }
+
+    SIP_HD static void write_slot(int tid, int s, float2* buf, const float2 (&A)[R], const float2 (&B)[R]) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) return;
+        const int q = f / U;
+        const int u = f - q * U;
+        float2* row = buf + q * K::LD;
+#pragma unroll
+        for (int r = 0; r < R; ++r) row[K::idx(u * R + r)] = A[r];
+        if (u != 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) row[K::idx((NR - u) * R + r)] = B[r];
+        }
+    }
+
+    struct Regs {
+        float2 a[S][R], b[S][R];
+    };
+
+    SIP_HD static void read(int tid, const TileArgs& a, const TileCtx& c, const float2* stage, Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) read_slot(tid, s, a, c, stage, rg.a[s], rg.b[s]);
+    }
+
+    SIP_HD static void write_smem(int tid, float2* buf, const Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) write_slot(tid, s, buf, rg.a[s], rg.b[s]);
+    }
+};
+
+// Type selection without the standard library (the run-time compiler has none).
+template <bool B, class T, class F>
+struct SkPick {
+    using type = T;
+};
+template <class T, class F>
+struct SkPick<false, T, F> {
+    using type = F;
+};
+
+// Pass 0 of a SK_SPLIT_PASS0 tile: from the staging buffer `stage` into the
+// work layout of the other buffer `work`, one slot at a time (no barrier
+// between reading and writing, so only one slot's values are live).
+template <class K>
+SIP_HD void sk_pass0_split(int tid, const TileArgs& a, const TileCtx& c, const float2* stage, float2* work) {
+    if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR)) {
+        using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
+#pragma unroll
+        for (int s = 0; s < PP::S; ++s) {
+            float2 A[PP::R], B[PP::R];
+            if (PP::read_slot(tid, s, a, c, stage, A, B)) PP::write_slot(tid, s, work, A, B);
+        }
+    } else {
+        using SP = SkPass<K, 0>;
+#pragma unroll
+        for (int s = 0; s < SP::S; ++s) {
+            float2 v[SP::R];
+            if (SP::read_slot(tid, s, a, c, stage, v)) SP::write_slot(tid, s, work, v);
+        }
+    }
+}
+
 // OP_PC: the spectra in the work layout times the filter spectrum, element
 // k of transform q times mul[(i0 + q) * mul_pitch_p + k * mul_pitch_k]
 // (conjugated under TF_MUL_CONJ), as tile_io.cuh mul_tile.
@@ -642,15 +1163,29 @@ __device__ __forceinline__ void sk_wait() {
 template <class K, int PASS>
 __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
     using SP = SkPass<K, PASS>;
-    typename SP::Regs rg;
-    SP::read(tid, a, c, buf, rg);
-    if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
-        SP::write_global(tid, a, c, rg);
+    if constexpr (K::MPAIR && K::OP == OP_R2C_HALF && SP::LAST) {
+        sk_pair_last_r2c<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_R2C_PAIR && SP::LAST) {
+        sk_pair_last_r2c_rows<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
+        using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
+        typename PP::Regs rg;
+        PP::read(tid, a, c, buf, rg);
+        __syncthreads();
+        PP::write_smem(tid, buf, rg);
+        __syncthreads();
+        sk_run<K, 1>(tid, a, c, buf);
     } else {
-        __syncthreads();
-        SP::write_smem(tid, buf, rg);
-        __syncthreads();
-        if constexpr (!SP::LAST) sk_run<K, PASS + 1>(tid, a, c, buf);
+        typename SP::Regs rg;
+        SP::read(tid, a, c, buf, rg);
+        if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
+            SP::write_global(tid, a, c, rg);
+        } else {
+            __syncthreads();
+            SP::write_smem(tid, buf, rg);
+            __syncthreads();
+            if constexpr (!SP::LAST) sk_run<K, PASS + 1>(tid, a, c, buf);
+        }
     }
 }
 
@@ -679,13 +1214,43 @@ __global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a)
     float2* bufs[2] = {sk_smem, sk_smem + (STAGES == 2 ? K::BUF : 0)};
     int tile = blockIdx.x;
     if (tile >= a.ntiles) return;
+    // staged twiddles after the buffers (the barrier before pass 0 of the
+    // first tile orders the copy before any use)
+    float2* tws = sk_smem + (STAGES == 2 ? 2 : 1) * K::BUF;
+    sk_load_tws<K>(tid, a, tws);
+    if constexpr (K::SPLIT) {
+        // buffers: bufs[0] stages the input, bufs[1] holds the work layout
+        static_assert(STAGES == 2, "a split pass 0 needs the staging and the work buffer");
+        sk_stage<K>(tid, a, decode_tile(a, tile), bufs[0]);
+        sk_commit();
+        for (; tile < a.ntiles; tile += gridDim.x) {
+            TileCtx c = decode_tile(a, tile);
+            if constexpr (K::TWS) c.tws = tws;
+            sk_wait<0>();
+            __syncthreads();
+            if constexpr (K::OP == OP_R2C_PAIR || K::OP == OP_C2R_PAIR) {
+                sk_zero_missing<K>(tid, a, c, bufs[0]);
+                __syncthreads();
+            }
+            sk_pass0_split<K>(tid, a, c, bufs[0], bufs[1]);
+            __syncthreads();
+            const int next = tile + gridDim.x;
+            if (next < a.ntiles) sk_stage<K>(tid, a, decode_tile(a, next), bufs[0]);
+            sk_commit();
+            sk_run<K, 1>(tid, a, c, bufs[1]);
+            if constexpr (sk_last_to_smem<K>()) sk_post<K>(tid, a, c, bufs[1]);
+            __syncthreads();
+        }
+        return;
+    }
     if (STAGES == 2) {
         sk_stage<K>(tid, a, decode_tile(a, tile), bufs[0]);
         sk_commit();
     }
     for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
         float2* cur = bufs[it & 1];
-        const TileCtx c = decode_tile(a, tile);
+        TileCtx c = decode_tile(a, tile);
+        if constexpr (K::TWS) c.tws = tws;
         if (STAGES == 2) {
             const int next = tile + gridDim.x;
             if (next < a.ntiles) sk_stage<K>(tid, a, decode_tile(a, next), bufs[(it + 1) & 1]);

@@ -11,6 +11,7 @@ struct SkEntry {
     int n, P, T, op, mode, sign;
     bool tw4;
     bool twb;  // basis pass twiddles (else the full Stockham table)
+    int flags = 1;  // the configuration's TWB bits (sk_kernel.cuh SK_TW_BASIS, SK_TW_SMEM, SK_MIRROR_PAIR)
     int stages;
     std::vector<int> radices;
     int LD;

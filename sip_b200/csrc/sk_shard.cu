@@ -24,10 +24,11 @@ SkEntry make_entry(std::vector<int> radices) {
     e.sign = K::SIGN;
     e.tw4 = K::TW4;
     e.twb = K::TWB;
+    e.flags = K::FLAGS;
     e.stages = STAGES;
     e.radices = std::move(radices);
     e.LD = K::LD;
-    e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8;
+    e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8 + K::TWSM * 8;
     e.fn = reinterpret_cast<const void*>(&sk_fft_kernel<K, STAGES>);
     e.minb = K::MINB;
     return e;

@@ -98,6 +98,9 @@ struct TileCtx {
     int cnt;   // transforms present in this tile (<= P)
     int i0;    // inner index of transform 0
     long long in_base, out_base;
+    // Twiddle tables staged in shared memory by the size-specialized kernels
+    // that keep them there (SK_TW_SMEM); null otherwise.
+    const float2* tws = nullptr;
 };
 
 SIP_HD TileCtx decode_tile(const TileArgs& a, int tile) {

@@ -286,13 +286,31 @@ class _GpuBase:
         return self.chirps[n]
 
     def filter(self, n: int):
-        """Spectrum of the zero-padded chirp (FP64 on the host, once per length)."""
+        """Spectrum of the zero-padded chirp, once per length: the chirp is
+        made on the device (FP64, rounded once) and transformed by the
+        library's own forward C2C plan, on the GPU."""
         if n not in self.filters:
-            from_host = np.zeros(n, np.complex128)
-            L = max(1, n // 4)
-            t = np.arange(L)
-            from_host[:L] = np.exp(1j * np.pi * t * t / L)
-            self.filters[n] = self.torch.from_numpy(np.fft.fft(from_host).astype(np.complex64)).to(self.dev)
+            from .fft import FftHandle, check
+            from . import _lib as L
+
+            torch = self.torch
+            Lc = max(1, n // 4)
+            t = torch.arange(Lc, dtype=torch.float64, device=self.dev)
+            c = torch.zeros(n, dtype=torch.complex64, device=self.dev)
+            c[:Lc] = torch.exp(1j * math.pi * t * t / Lc).to(torch.complex64)
+            spec = torch.empty_like(c)
+            torch.cuda.synchronize(self.dev)  # the chirp, made on torch's stream
+            h = FftHandle()
+            try:
+                check(h.make_plan_1d(n, L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, 1), "filter plan")
+                h.bind_workspace(self.dev)
+                s = self.streams[0]
+                check(h.set_stream(s), "filter stream")
+                check(h.exec_raw(c.data_ptr(), spec.data_ptr()), "filter exec")
+                s.synchronize()
+            finally:
+                h.destroy()
+            self.filters[n] = spec
         return self.filters[n]
 
     def make_signal(self, r: Request, x) -> None:

@@ -43,6 +43,8 @@ def load():
     lib.emu_radices.restype = c.c_int
     lib.emu_dft.argtypes = [c.c_int, c.c_int, c.c_void_p]
     lib.emu_dft.restype = c.c_int
+    lib.emu_set_chunk_bytes.argtypes = [c.c_longlong]
+    lib.emu_set_chunk_bytes.restype = None
     return lib
 
 

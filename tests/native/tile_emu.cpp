@@ -10,6 +10,7 @@
 // Shared memory is filled with NaN before each tile so a read of a slot no
 // phase wrote shows up in the result.  Twiddles are computed on the host
 // in long double and rounded once to float.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -120,13 +121,25 @@ void emu_passes(int T, const TileArgs& a, float2* sm) {
 template <class K, int PASS>
 void emu_sk_passes(const TileArgs& a, const TileCtx& c, float2* buf) {
     using SP = SkPass<K, PASS>;
-    std::vector<typename SP::Regs> regs(K::T);
-    for (int tid = 0; tid < K::T; ++tid) SP::read(tid, a, c, buf, regs[tid]);
-    if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
-        for (int tid = 0; tid < K::T; ++tid) SP::write_global(tid, a, c, regs[tid]);
+    if constexpr (K::MPAIR && K::OP == OP_R2C_HALF && SP::LAST) {
+        for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_R2C_PAIR && SP::LAST) {
+        for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c_rows<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
+        using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
+        std::vector<typename PP::Regs> regs(K::T);
+        for (int tid = 0; tid < K::T; ++tid) PP::read(tid, a, c, buf, regs[tid]);
+        for (int tid = 0; tid < K::T; ++tid) PP::write_smem(tid, buf, regs[tid]);
+        emu_sk_passes<K, 1>(a, c, buf);
     } else {
-        for (int tid = 0; tid < K::T; ++tid) SP::write_smem(tid, buf, regs[tid]);
-        if constexpr (!SP::LAST) emu_sk_passes<K, PASS + 1>(a, c, buf);
+        std::vector<typename SP::Regs> regs(K::T);
+        for (int tid = 0; tid < K::T; ++tid) SP::read(tid, a, c, buf, regs[tid]);
+        if constexpr (SP::LAST && !sk_last_to_smem<K>()) {
+            for (int tid = 0; tid < K::T; ++tid) SP::write_global(tid, a, c, regs[tid]);
+        } else {
+            for (int tid = 0; tid < K::T; ++tid) SP::write_smem(tid, buf, regs[tid]);
+            if constexpr (!SP::LAST) emu_sk_passes<K, PASS + 1>(a, c, buf);
+        }
     }
 }
 
@@ -134,11 +147,23 @@ template <class K>
 void emu_sk_run(const TileArgs& a) {
     const float nan = std::numeric_limits<float>::quiet_NaN();
     std::vector<float2> buf(K::BUF);
+    // staged twiddles (SK_TW_SMEM), NaN where the copy does not write
+    std::vector<float2> tws(K::TWSM + 1, make_float2(nan, nan));
+    for (int tid = 0; tid < K::T; ++tid) sk_load_tws<K>(tid, a, tws.data());
     for (int tile = 0; tile < a.ntiles; ++tile) {
-        const TileCtx c = decode_tile(a, tile);
+        TileCtx c = decode_tile(a, tile);
+        if constexpr (K::TWS) c.tws = tws.data();
         for (auto& v : buf) v = make_float2(nan, nan);
         for (int tid = 0; tid < K::T; ++tid) sk_stage<K>(tid, a, c, buf.data());
         for (int tid = 0; tid < K::T; ++tid) sk_zero_missing<K>(tid, a, c, buf.data());
+        if constexpr (K::SPLIT) {  // pass 0 from the staging buffer into a separate work buffer
+            std::vector<float2> work(K::BUF, make_float2(nan, nan));
+            for (int tid = 0; tid < K::T; ++tid) sk_pass0_split<K>(tid, a, c, buf.data(), work.data());
+            emu_sk_passes<K, 1>(a, c, work.data());
+            if constexpr (sk_last_to_smem<K>())
+                for (int tid = 0; tid < K::T; ++tid) sk_post<K>(tid, a, c, work.data());
+            continue;
+        }
         if constexpr (K::OP == OP_PC) {
             emu_sk_passes<SkView<K, OP_PC, -1, false>, 0>(a, c, buf.data());
             for (int tid = 0; tid < K::T; ++tid) sk_mul<K>(tid, a, c, buf.data());
@@ -164,10 +189,11 @@ SkEntry emu_entry(std::vector<int> radices) {
     e.sign = K::SIGN;
     e.tw4 = K::TW4;
     e.twb = K::TWB;
+    e.flags = K::FLAGS;
     e.stages = STAGES;
     e.radices = std::move(radices);
     e.LD = K::LD;
-    e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8;
+    e.smem = (STAGES == 2 ? 2 : 1) * K::BUF * 8 + K::TWSM * 8;
     e.fn = reinterpret_cast<const void*>(&emu_sk_run<K>);
     return e;
 }
@@ -442,34 +468,65 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
     }
     if (desc && desc_cap) std::snprintf(desc, desc_cap, "%s", describe(p).c_str());
     try {
-        std::vector<char> ws(p.workspace_need + 16);
-        for (const Step& st : p.steps) {
+        // NaN-filled workspace: a chunk that read what no step of it wrote
+        // would show up in the result
+        std::vector<float> wsf((p.workspace_need + 16) / 4 + 1, std::numeric_limits<float>::quiet_NaN());
+        char* ws = reinterpret_cast<char*>(wsf.data());
+        // one step, restricted to chunk units [u0, u0 + cnt) of its group
+        // when cnt >= 0 (the launch_steps order of the library)
+        auto run_step = [&](const Step& st, long long u0, long long cnt, int lane, long long cu) {
             auto resolve = [&](Loc l, size_t off) -> char* {
                 char* base = l == Loc::In ? const_cast<char*>(static_cast<const char*>(in))
-                           : l == Loc::Out ? static_cast<char*>(out) : ws.data();
+                           : l == Loc::Out ? static_cast<char*>(out) : ws;
                 return base + off;
             };
             char* s = resolve(st.src, st.src_off);
             char* d = resolve(st.dst, st.dst_off);
             std::vector<float2> filt;
-            Step stc;
-            const Step* use = &st;
+            Step stc = st;
+            if (cnt >= 0) {
+                s += chunk_offset(st, true, u0, lane, cu);
+                d += chunk_offset(st, false, u0, lane, cu);
+                if (st.kind == StepKind::Tile) stc.L = chunk_tile_launch(st, cnt);
+                else stc.real.rows = cnt * st.chunk_per;
+            }
             if (st.mul_table == 1) {  // the Bluestein filter the device preparation would make
                 filt = bluestein_filter(st.blue_n, st.blue_m, st.blue_sign);
-                stc = st;
                 stc.L.args.mul = filt.data();
-                use = &stc;
             }
             if (st.kind == StepKind::Blue) emu_blue_step(st, s, d);
-            else if (use->kind == StepKind::Tile) emu_tile_step(*use, s, d);
+            else if (st.kind == StepKind::Tile) emu_tile_step(stc, s, d);
             else if (st.kind == StepKind::Tc) emu_tc_step(st, s, d);
-            else emu_real_step(st, s, d);
+            else emu_real_step(stc, s, d);
+        };
+        for (size_t i = 0; i < p.steps.size();) {
+            const int gi = p.steps[i].chunk_group;
+            if (gi >= 0) {
+                const ChunkGroup& g = p.chunk_groups[gi];
+                const long long cu = chunk_units(g);
+                if (cu < g.units) {
+                    // the library's lanes: chunk k on lane k % 2 (workspace
+                    // regions per lane); run in order here
+                    int k = 0;
+                    for (long long u0 = 0; u0 < g.units; u0 += cu, ++k)
+                        for (size_t j = g.first; j < g.last; ++j)
+                            run_step(p.steps[j], u0, std::min(cu, g.units - u0), chunk_lanes() == 2 ? (k & 1) : 0, cu);
+                    i = g.last;
+                    continue;
+                }
+            }
+            run_step(p.steps[i], 0, -1, 0, 0);
+            ++i;
         }
     } catch (const std::exception&) {
         return -1;
     }
     return 0;
 }
+
+// Chunk size of the L2-resident chunks for plans made afterwards (bytes;
+// 0 off, negative: the library default).
+void emu_set_chunk_bytes(long long bytes) { set_l2_chunk_bytes(bytes); }
 
 // Fast-division check: returns the number of mismatches of fd_div against
 // exact division over `count` (divisor, dividend) pairs.

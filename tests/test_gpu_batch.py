@@ -72,9 +72,10 @@ def jobs(cuda):
 
 
 def oracle_check(job, out):
+    # the library's accuracy bar, as for the plain exec
     op, d, sizes, b = job.case
     want = O.fp64(op, d, job.x, sizes)
-    assert O.rel_l2(out, want) < 2e-6, job.case
+    assert O.rel_l2(out, want) <= 1e-6, job.case
 
 
 def test_mix_equals_alone_and_plain(cuda, jobs):

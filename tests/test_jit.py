@@ -305,3 +305,30 @@ plan(4320)                      # leave one running at exit
     r = subprocess.run([sys.executable, "-W", "ignore", "-c", code], env=env, capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+def test_exit_while_compiling_many_times(tmp_path):
+    """Processes that exit a fraction of a second after starting background
+    compilations (four steps, cold cache) exit cleanly every time.  Before the
+    compiler was warmed up ahead of the exit-time drain, some of these exits
+    crashed: the compiler's own teardown ran while a worker still compiled."""
+    import subprocess
+    import sys
+
+    if not _nvrtc_present():
+        pytest.skip("NVRTC not available")
+    code = r'''
+import sys, time
+sys.path.insert(0, %r)
+from sip_b200 import _lib as L
+from sip_b200.fft import FftHandle
+for n, b in ((1 << 21, 64), (184320, 16)):   # four-step lengths without compiled kernels
+    h = FftHandle()
+    assert h.make_plan_1d(n, L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, b) == 0
+time.sleep(float(sys.argv[1]))
+''' % os.getcwd()
+    for i, delay in enumerate((0.0, 0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.7)):
+        env = dict(os.environ, SIP_FFT_JIT_CACHE=str(tmp_path / f"jit{i}"))
+        r = subprocess.run([sys.executable, "-W", "ignore", "-c", code, str(delay)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, (delay, r.returncode, r.stderr[-2000:])
