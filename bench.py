@@ -53,6 +53,15 @@ def bytes_real(n: int, rows: int) -> int:
     return rows * (4 * n + 8 * (n // 2 + 1))
 
 
+def kernel_config(desc: dict) -> str:
+    """The size-specialized kernel of a one-step plan, spelled as its
+    template arguments (SkCfg<N,P,T,OP,MODE,SIGN,TW4,MINB,TWB,radices...>)."""
+    steps = desc["steps"]
+    if len(steps) != 1 or "sk_cfg" not in steps[0]:
+        return ""
+    return "SkCfg<" + ",".join(str(v) for v in steps[0]["sk_cfg"] + steps[0]["radices"]) + ">"
+
+
 def load_peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -610,7 +619,8 @@ def run_ours(args) -> None:
         # the reference's exec entry points on aclTensor descriptors, made once
         acl = (create_acl_tensor(x), create_acl_tensor(spec), create_acl_tensor(y))
         plans.append(dict(n=n, rows=rows, x=x, spec=spec, y=y, hr=hr, hc=hc, kernels=(kr, kc), acl=acl,
-                          steps=(len(hr.describe()["steps"]), len(hc.describe()["steps"]))))
+                          steps=(len(hr.describe()["steps"]), len(hc.describe()["steps"])),
+                          cfg=(kernel_config(hr.describe()), kernel_config(hc.describe()))))
     torch.cuda.synchronize()
     lib = L.lib()
 
@@ -679,21 +689,25 @@ def run_ours(args) -> None:
     peak, peak_kind = load_peaks()
     cands = []
     for p, r2c, c2r in per:
-        for name, ms, k, ns in (("r2c", r2c, p["kernels"][0], p["steps"][0]), ("c2r", c2r, p["kernels"][1], p["steps"][1])):
+        for name, ms, k, ns, cfg in (("r2c", r2c, p["kernels"][0], p["steps"][0], p["cfg"][0]),
+                                     ("c2r", c2r, p["kernels"][1], p["steps"][1], p["cfg"][1])):
             gbs = bytes_real(p["n"], p["rows"]) / (ms * 1e-3) / 1e9
             cands.append(dict(exec=f"{name} N={p['n']} rows={p['rows']}", kernels=k, steps=ns, ms=float(f"{ms:.4f}"),
                               gbs=round(gbs, 1), frac=round(gbs / peak, 4),
-                              bytes=bytes_real(p["n"], p["rows"])))
+                              bytes=bytes_real(p["n"], p["rows"]), kernel=cfg))
     single = [c for c in cands if c["kernels"] == 1 and c["steps"] == 1]
     dom = max(single or cands, key=lambda c: c["ms"])
+    # DRAM traffic of the dominant kernel from an ncu capture recorded in
+    # profiles/dram_traffic.md; used only when the recorded kernel
+    # configuration is the one this run executed (else null)
     traffic = None
     tfile = ROOT / "profiles" / "dram_traffic.md"
     if tfile.exists():
         key = dom["exec"].split(" rows")[0]
         for line in tfile.read_text().splitlines():
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if len(cells) >= 2 and cells[0] == key and cells[1].isdigit():
-                traffic = int(cells[1])
+            cells = [c.strip().strip("`") for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 3 and cells[0] == key and cells[1] == dom["kernel"] and cells[2].isdigit():
+                traffic = int(cells[2])
 
     # end to end through the C ABI from pinned host memory
     e2e = None
@@ -745,8 +759,8 @@ def run_ours(args) -> None:
             "gflops_2_5nlogn": round(world * step_flops25 / (ms_per_step * 1e-3) / 1e9, 3),
             "hbm_gbs_step": round(world * step_bytes / (ms_per_step * 1e-3) / 1e9, 1),
             "roofline": {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
-                         "traffic": traffic, "kernel": dom["exec"], "algorithmic_bytes": dom["bytes"],
-                         "peak_kind": peak_kind},
+                         "traffic": traffic, "kernel": dom["exec"], "kernel_config": dom["kernel"],
+                         "algorithmic_bytes": dom["bytes"], "peak_kind": peak_kind},
             "execs": cands,
             "parity": parity,
             "e2e": e2e,

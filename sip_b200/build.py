@@ -79,12 +79,29 @@ def _newest_header() -> float:
     return max((h.stat().st_mtime for h in heads), default=0.0)
 
 
+def _deps_mtime(dep: Path, head_mtime: float) -> float:
+    """Newest mtime of the headers a unit included at its last compile (the
+    compiler's dependency file); every header when there is none."""
+    if not dep.exists():
+        return head_mtime
+    text = dep.read_text().replace("\\\n", " ")
+    names = text.split(":", 1)[1].split() if ":" in text else []
+    newest = 0.0
+    for n in names:
+        p = Path(n)
+        if not p.exists():
+            return head_mtime  # a header went away: rebuild
+        newest = max(newest, p.stat().st_mtime)
+    return newest
+
+
 def _compile(src: str, defs: list[str], obj: str, head_mtime: float, verbose: bool) -> str:
     out = BUILD / obj
+    dep = BUILD / (obj + ".d")
     s = CSRC / src  # an absolute src (generated under _build) replaces CSRC
-    if out.exists() and out.stat().st_mtime >= max(s.stat().st_mtime, head_mtime):
+    if out.exists() and out.stat().st_mtime >= max(s.stat().st_mtime, _deps_mtime(dep, head_mtime)):
         return f"up to date {obj}"
-    cmd = [NVCC, *ARCH, *COMMON, *defs, "-c", str(s), "-o", str(out)]
+    cmd = [NVCC, *ARCH, *COMMON, *defs, "-MD", "-MF", str(dep), "-c", str(s), "-o", str(out)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -33,6 +33,24 @@ __global__ void k_chirp(float2* out, long long n, int sign) {
     }
 }
 
+// The convolution sequence of the Bluestein filter: b_j = conj(c_j) for
+// j < n and b_{m-j} = b_j for 0 < j < n, zero elsewhere (m >= 2n - 1); the
+// filter is its length-m FFT.  FP64 phases, rounded once.
+__global__ void k_blue_b(float2* out, long long n, long long m, int sign) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long j = i < n ? i : (i > m - n ? m - i : -1);
+        if (j < 0) {
+            out[i] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const long long q = (j * j) % (2 * n);
+        double s, c;
+        sincospi((double)q / (double)n, &s, &c);
+        out[i] = make_float2((float)c, (float)(-sign * s));
+    }
+}
+
 dim3 grid2(long long per_row, long long rows) {
     long long gx = (per_row + kBlueBlock - 1) / kBlueBlock;
     if (gx > 4096) gx = 4096;
@@ -56,6 +74,13 @@ cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream) {
 
 cudaError_t bluestein_post(const BluesteinArgs& a, cudaStream_t stream) {
     k_blue_post<<<grid2(blue_out_count(a), a.rows), kBlueBlock, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t gen_blue_b(float2* out, long long n, long long m, int sign, cudaStream_t stream) {
+    long long g = (m + kBlueBlock - 1) / kBlueBlock;
+    if (g > 65535) g = 65535;
+    k_blue_b<<<(unsigned)g, kBlueBlock, 0, stream>>>(out, n, m, sign);
     return cudaGetLastError();
 }
 

@@ -141,15 +141,51 @@ BufPtr chirp_table(int device, long long n, int sign) {
     return b;
 }
 
+// Filter of a long Bluestein convolution made on the GPU: the sequence b in
+// FP64 (rounded once), then the library's own forward C2C plan of length m
+// (2,3,5-smooth, so it never needs Bluestein itself) in FP32.
+BufPtr blue_filter_gpu(int device, long long n, long long m, int sign) {
+    BufPtr seq = alloc_buf((size_t)m * sizeof(float2), device);
+    BufPtr out = alloc_buf((size_t)m * sizeof(float2), device);
+    run_sync([&](cudaStream_t s) { return gen_blue_b(static_cast<float2*>(seq->ptr), n, m, sign, s); });
+    FftPlan p;
+    p.type = AsdSip::ASCEND_FFT_C2C;
+    p.direction = AsdSip::ASCEND_FFT_FORWARD;
+    p.sizes = {m};
+    p.batch = 1;
+    build_steps(p);
+    prepare_device(p);
+    BufPtr ws = alloc_buf(p.workspace_need, device);
+    run_sync([&](cudaStream_t s) {
+        p.stream = s;
+        launch_steps(p, seq->ptr, out->ptr, ws->ptr);
+        return cudaGetLastError();
+    });
+    return out;
+}
+
 BufPtr blue_filter_table(int device, long long n, long long m, int sign) {
     TableKey key{device, 6, n, m * 2 + (sign > 0 ? 1 : 0), {}};
+    {
+        std::lock_guard<std::mutex> lk(g_table_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end())
+            if (auto sp = it->second.lock()) return sp;
+    }
+    // made without the table lock: the GPU form prepares a plan of its own,
+    // whose twiddle tables go through the same cache
+    BufPtr b;
+    if (m > kHostBlueFilterMax) {
+        b = blue_filter_gpu(device, n, m, sign);
+    } else {
+        const std::vector<float2> host = bluestein_filter(n, m, sign);
+        b = alloc_buf(host.size() * sizeof(float2), device);
+        check(cudaMemcpy(b->ptr, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice), "cudaMemcpy");
+    }
     std::lock_guard<std::mutex> lk(g_table_mu);
     auto it = g_tables.find(key);
     if (it != g_tables.end())
-        if (auto sp = it->second.lock()) return sp;
-    const std::vector<float2> host = bluestein_filter(n, m, sign);
-    BufPtr b = alloc_buf(host.size() * sizeof(float2), device);
-    check(cudaMemcpy(b->ptr, host.data(), host.size() * sizeof(float2), cudaMemcpyHostToDevice), "cudaMemcpy");
+        if (auto sp = it->second.lock()) return sp;  // made by another thread meanwhile
     g_tables[key] = b;
     return b;
 }

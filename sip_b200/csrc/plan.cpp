@@ -618,7 +618,9 @@ bool real_direct(long long n) {
     return n <= kMaxTileN && factorizable((int)n, 32);
 }
 
-constexpr long long kMaxBluesteinN = 1LL << 22;
+// Bluestein up to the reference's largest length (fft_api.cpp:82): the
+// convolution length m <= 2^28 splits into two passes of at most 16384.
+constexpr long long kMaxBluesteinN = 1LL << 27;
 
 // Bluestein's algorithm (bluestein.cuh): pre pass into the workspace, the
 // fused pulse chain of length m in place there (filter = the plan's
@@ -634,7 +636,7 @@ struct BlueIO {
 
 void add_bluestein(FftPlan& plan, int kind, long long n, long long batch, const BlueIO& io = BlueIO{}) {
     if (n > kMaxBluesteinN)
-        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " needs Bluestein above 2^22");
+        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "length " + std::to_string(n) + " needs Bluestein above 2^27");
     const long long m = bluestein_length(n);
     const int sign = io.sign != 0 ? io.sign : (plan.forward() ? -1 : 1);
     if (kind == BLUE_C2C && m <= kMaxTileN) {
@@ -1344,7 +1346,12 @@ std::string describe(const FftPlan& plan) {
                << ",\"flags\":" << a.flags << ",\"inner\":" << a.inner << ",\"tiles_per_outer\":" << a.tiles_per_outer
                << ",\"in\":[" << a.in_odist << "," << a.in_idist << "," << a.in_stride << "],\"out\":["
                << a.out_odist << "," << a.out_idist << "," << a.out_stride << "],\"sk\":" << (st.sk ? "true" : "false")
-               << ",\"jit\":" << (st.sk && st.sk->jit ? "true" : "false") << ",\"radices\":[";
+               << ",\"jit\":" << (st.sk && st.sk->jit ? "true" : "false");
+            if (st.sk)  // the compiled configuration (SkCfg<N, P, T, OP, MODE, SIGN, TW4, MINB, TWB, radices>)
+                os << ",\"sk_cfg\":[" << st.sk->n << "," << st.sk->P << "," << st.sk->T << "," << st.sk->op << ","
+                   << st.sk->mode << "," << st.sk->sign << "," << (st.sk->tw4 ? 1 : 0) << "," << st.sk->minb << ","
+                   << st.sk->flags << "]";
+            os << ",\"radices\":[";
             for (size_t r = 0; r < st.radices.size(); ++r) os << (r ? "," : "") << st.radices[r];
             os << "]";
         } else if (st.kind == StepKind::Blue) {

@@ -13,17 +13,17 @@
 #pragma once
 
 #define SIP_SK_CONFIGS(X)                                                     \
-    /* 1D / last-axis C2C rows */                                             \
+    /* 1D / last-axis C2C rows (split pass 0, TWB 9) */                       \
     X(0, 4096, 1, 128, OP_C2C, SK_ROWS, -1, false, 2, 3, 9, 16, 16, 16)              \
     X(1, 4096, 1, 128, OP_C2C, SK_ROWS, 1, false, 2, 3, 9, 16, 16, 16)               \
-    X(2, 2048, 2, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 8)               \
-    X(3, 2048, 2, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 8)                \
-    X(4, 1024, 4, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16, 4)               \
-    X(5, 1024, 4, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16, 4)                \
-    X(6, 256, 16, 256, OP_C2C, SK_ROWS, -1, false, 2, 3, 1, 16, 16)                  \
-    X(7, 256, 16, 256, OP_C2C, SK_ROWS, 1, false, 2, 3, 1, 16, 16)                   \
-    X(0, 8192, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 1, 1, 32, 16, 16)              \
-    X(1, 8192, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 1, 1, 32, 16, 16)               \
+    X(2, 2048, 1, 128, OP_C2C, SK_ROWS, -1, false, 2, 4, 9, 16, 16, 8)               \
+    X(3, 2048, 1, 128, OP_C2C, SK_ROWS, 1, false, 2, 4, 9, 16, 16, 8)                \
+    X(4, 1024, 4, 256, OP_C2C, SK_ROWS, -1, false, 2, 2, 9, 16, 16, 4)               \
+    X(5, 1024, 4, 256, OP_C2C, SK_ROWS, 1, false, 2, 2, 9, 16, 16, 4)                \
+    X(6, 256, 8, 128, OP_C2C, SK_ROWS, -1, false, 2, 4, 9, 16, 16)                   \
+    X(7, 256, 8, 128, OP_C2C, SK_ROWS, 1, false, 2, 4, 9, 16, 16)                    \
+    X(0, 8192, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 1, 9, 32, 16, 16)              \
+    X(1, 8192, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 1, 9, 32, 16, 16)               \
     /* strided axes of 2D / 3D transforms */                                  \
     X(2, 2048, 8, 512, OP_C2C, SK_COLS, -1, false, 1, 1, 1, 16, 16, 8)               \
     X(3, 2048, 8, 512, OP_C2C, SK_COLS, 1, false, 1, 1, 1, 16, 16, 8)                \
@@ -48,7 +48,8 @@
     X(0, 500, 2, 64, OP_R2C_HALF, SK_ROWS, -1, false, 2, 8, 15, 25, 5, 4)            \
     X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 5, 10, 10)           \
     X(2, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 15, 25, 15, 8)         \
-    X(3, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 9, 25, 8, 15)           \
+    X(3, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 15, 15, 8, 25)          \
+    X(7, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 9, 25, 8, 15)           \
     X(4, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 7, 15, 25, 8)          \
     X(5, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 8, 15)           \
     /* real rows of N = 2048, 4096, 8192 (half lengths 1024, 2048, 4096) */  \
@@ -77,6 +78,22 @@
        (planner hint) */                                                     \
     X(4, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 1, 32, 32)            \
     X(5, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 3, 1, 16, 32)                \
+    /* hint variants of the multi-pass steps: split pass 0 (TWB 8) or more, \
+       smaller CTAs per SM */                                                 \
+    X(0, 1024, 8, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 3, 32, 32)             \
+    X(1, 1024, 4, 128, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 3, 11, 32, 32)            \
+    X(2, 512, 8, 128, OP_C2C, SK_COLS, -1, true, 2, 3, 9, 16, 32)                   \
+    X(3, 512, 8, 128, OP_C2C, SK_COLS, 1, true, 2, 3, 9, 16, 32)                    \
+    X(4, 1024, 4, 128, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 9, 32, 32)                \
+    X(5, 1024, 4, 128, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 9, 32, 32)                 \
+    X(6, 256, 16, 256, OP_C2C, SK_COLS, -1, true, 2, 3, 9, 16, 16)                   \
+    X(7, 256, 16, 256, OP_C2C, SK_COLS, 1, true, 2, 3, 9, 16, 16)                    \
+    X(0, 256, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 9, 16, 16)                \
+    X(1, 256, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 9, 16, 16)                 \
+    X(2, 256, 16, 256, OP_C2C, SK_COLS, -1, false, 2, 3, 9, 16, 16)                  \
+    X(3, 256, 16, 256, OP_C2C, SK_COLS, 1, false, 2, 3, 9, 16, 16)                   \
+    X(4, 2048, 4, 256, OP_C2C, SK_COLS, -1, false, 1, 3, 1, 16, 16, 8)               \
+    X(5, 2048, 4, 256, OP_C2C, SK_COLS, 1, false, 1, 3, 1, 16, 16, 8)                \
     /* the C2R form with mirrored pairs in its split pass 0: a hint variant  \
        (slower than the plain split pass for N = 6000) */                   \
     X(6, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 15, 25, 8)          \

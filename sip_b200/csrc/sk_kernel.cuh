@@ -64,7 +64,7 @@ SIP_HD constexpr int sk_tws_stride(int op, int flags, int p, int np, int L) {
 SIP_HD constexpr int sk_tw2s(int op, int n, int r0, int rlast, int flags) {
     return !(flags & SK_TW_SMEM) ? 0
          : op == OP_R2C_HALF ? ((flags & SK_MIRROR_PAIR) ? n / rlast / 2 + 1 : n / 2 + 1)
-         : op == OP_C2R_HALF ? ((flags & SK_MIRROR_PAIR) ? n / r0 / 2 + 1 : n)
+         : op == OP_C2R_HALF ? ((flags & SK_MIRROR_PAIR) ? n / r0 / 2 + 1 : n / r0)
          : 0;
 }
 // Complex values of shared memory the staged twiddles take (even count).
@@ -498,6 +498,20 @@ SIP_HD float2 sk_input(const TileArgs& a, const TileCtx& c, const float2* stage,
     }
 }
 
+// Compile-time loop: f(SkIC<I>{}) for I in [B, E), so that the index can be a
+// template argument (the compile-time roots of tw_const).
+template <int V>
+struct SkIC {
+    static constexpr int value = V;
+};
+template <int I, int E, class F>
+SIP_HD void sk_static_for(F&& f) {
+    if constexpr (I < E) {
+        f(SkIC<I>{});
+        sk_static_for<I + 1, E>(f);
+    }
+}
+
 // ------------------------------------------------------------- passes
 template <class K, int PASS>
 struct SkPass {
@@ -528,12 +542,35 @@ struct SkPass {
         if (TOTAL % K::T != 0 && b >= TOTAL) return false;
         int q, j;
         butterfly_index(b, q, j);
+        if constexpr (PASS == 0 && !K::WORK_IN && K::OP == OP_C2R_HALF) {
+            // C2R pre-process: the twiddle of element n = j + r NR is
+            // W_{2M}^{j + r NR} = W_{2M}^j W_{2R}^r, one table entry per
+            // butterfly times compile-time constants
+            const float2 wj = sk_tw2<K>(a, c, j);
+            const float2* row = buf + q * (K::N + 1);
+            const bool cj = (a.flags & TF_CONJ_IN) != 0;
+            sk_static_for<0, R>([&](auto ic) {
+                constexpr int r = decltype(ic)::value;
+                const int n = j + r * NR;
+                if (n == 0) {
+                    const float dc = row[0].x, ny = row[K::N].x;
+                    v[r] = make_float2(0.5f * (dc + ny), 0.5f * (dc - ny));
+                } else {
+                    const float2 x = maybe_conj(row[n], cj), y = maybe_conj(row[K::N - n], cj);
+                    const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+                    const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
+                    const float2 od = c_mulc(d, tw_const<2 * R, r, -1>(wj));
+                    v[r] = make_float2(e.x - od.y, e.y + od.x);
+                }
+            });
+        } else {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if constexpr (PASS == 0 && !K::WORK_IN)
-                v[r] = sk_input<K>(a, c, buf, q, j + r * NR);
-            else
-                v[r] = buf[q * K::LD + K::idx(j + r * NR)];
+            for (int r = 0; r < R; ++r) {
+                if constexpr (PASS == 0 && !K::WORK_IN)
+                    v[r] = sk_input<K>(a, c, buf, q, j + r * NR);
+                else
+                    v[r] = buf[q * K::LD + K::idx(j + r * NR)];
+            }
         }
         if constexpr (L > 1) {
             // twiddle-major tables: consecutive k of a warp read consecutive
@@ -753,20 +790,6 @@ SIP_HD void sk_post(int tid, const TileArgs& a, const TileCtx& c, const float2* 
 // real twiddles W_{2M}^{u + r NR} = W_{2M}^u W_{2R}^r need table entries of
 // u only, times compile-time constants.
 
-// Compile-time loop: f(SkIC<I>{}) for I in [B, E), so that the index can be a
-// template argument (the compile-time roots of tw_const).
-template <int V>
-struct SkIC {
-    static constexpr int value = V;
-};
-template <int I, int E, class F>
-SIP_HD void sk_static_for(F&& f) {
-    if constexpr (I < E) {
-        f(SkIC<I>{});
-        sk_static_for<I + 1, E>(f);
-    }
-}
-
 // Last pass of an R2C_HALF tile, post-process fused, output to global memory.
 template <class K>
 SIP_HD void sk_pair_last_r2c(int tid, const TileArgs& a, const TileCtx& c, const float2* buf) {
@@ -869,38 +892,26 @@ struct SkPairFirstC2R {
         const int u = f - q * U;
         const float2* row = stage + q * (M + 1);
         const float2 wu = sk_tw2<K>(a, c, u);
-        {
-            if (u == 0) {
-                const float dc = row[0].x, ny = row[M].x;
-                A[0] = make_float2(0.5f * (dc + ny), 0.5f * (dc - ny));
-                sk_static_for<1, R / 2 + 1>([&](auto ic) {
-                    constexpr int r = decltype(ic)::value;
-                    const int n = r * NR;
-                    float2 zn, zm;
-                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), zn, zm);
-                    A[r] = zn;
-                    if (2 * r != R) A[R - r] = zm;
-                });
-            } else if (2 * u == NR) {
-                sk_static_for<0, (R + 1) / 2>([&](auto ic) {
-                    constexpr int r = decltype(ic)::value;
-                    const int n = u + r * NR;
-                    float2 zn, zm;
-                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), zn, zm);
-                    A[r] = zn;
-                    if (2 * r + 1 != R) A[R - 1 - r] = zm;
-                });
-            } else {
-                sk_static_for<0, R>([&](auto ic) {
-                    constexpr int r = decltype(ic)::value;
-                    const int n = u + r * NR;
-                    prep(maybe_conj(row[n], cj), maybe_conj(row[M - n], cj), tw_const<2 * R, r, -1>(wu), A[r],
-                         B[R - 1 - r]);
-                });
-                dft<R, K::SIGN>(B);
+        // One code path for every unit: element r of butterfly u is Z[n] from
+        // (X[n], X[M - n]), n = u + r NR, and the same pair gives element
+        // R - 1 - r of the mirror butterfly.  For u = 0 (and u = NR / 2) the
+        // mirror is the butterfly itself, whose elements all come out of the
+        // Z[n] side (each of its bins is read twice there); X[0] and X[M] enter
+        // with their imaginary parts ignored, which turns the formula into
+        // Z[0] = ((X0 + XM) / 2, (X0 - XM) / 2).
+        const bool mirror = u != 0 && 2 * u != NR;
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            const int n = u + r * NR;
+            float2 x = maybe_conj(row[n], cj), y = maybe_conj(row[M - n], cj);
+            if (n == 0) {
+                x.y = 0.f;
+                y.y = 0.f;
             }
-            dft<R, K::SIGN>(A);
-        }
+            prep(x, y, tw_const<2 * R, r, -1>(wu), A[r], B[R - 1 - r]);
+        });
+        if (mirror) dft<R, K::SIGN>(B);
+        dft<R, K::SIGN>(A);
         return true;
     }
 
@@ -1040,31 +1051,17 @@ struct SkPairFirstC2RRows {
         const int u = f - q * U;
         const float2* sa = stage + (2 * q) * H;
         const float2* sb = sa + H;
-        if (u == 0) {
-            sk_static_for<0, R / 2 + 1>([&](auto ic) {
-                constexpr int r = decltype(ic)::value;
-                float2 lo, hi;
-                bins(sa, sb, r * NR, fwd, lo, hi);
-                A[r] = lo;
-                if (r != 0) A[R - r] = hi;
-            });
-        } else {
-            sk_static_for<0, R>([&](auto ic) {
-                constexpr int r = decltype(ic)::value;
-                const int n = u + r * NR;
-                float2 lo, hi;
-                if (2 * n < N) {
-                    bins(sa, sb, n, fwd, lo, hi);
-                    A[r] = lo;
-                    B[R - 1 - r] = hi;
-                } else {
-                    bins(sa, sb, N - n, fwd, lo, hi);
-                    A[r] = hi;
-                    B[R - 1 - r] = lo;
-                }
-            });
-            dft<R, K::SIGN>(B);
-        }
+        // one code path for every unit (u = 0 is its own mirror: B unused)
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            const int n = u + r * NR;
+            const bool low = 2 * n < N;
+            float2 lo, hi;
+            bins(sa, sb, low ? n : N - n, fwd, lo, hi);
+            A[r] = low ? lo : hi;
+            B[R - 1 - r] = low ? hi : lo;
+        });
+        if (u != 0) dft<R, K::SIGN>(B);
         dft<R, K::SIGN>(A);
         return true;
     }

@@ -235,6 +235,10 @@ def test_partial_overlap_rejected(sip_lib, handle):
     (R2C, [1 << 20], ["four-step A", "r2c four-step B + post"]),
     (C2R, [1 << 20], ["c2r pre", "four-step A", "four-step B"]),
     (C2R, [64, 64], ["c2c axis 0", "c2r half"]),
+    # Bluestein up to the largest length (2^27): a convolution of 2^28 in
+    # the four-step pulse chain
+    (C2C, [(1 << 27) - 1], ["bluestein pre", "four-step A", "pulse rows", "pulse inverse columns",
+                            "bluestein post"]),
 ])
 def test_plan_steps(sip_lib, handle, t, sizes, kinds):
     """Every axis is one pass (no transposes); four-step above one tile."""
@@ -331,3 +335,13 @@ def test_real_fused_hint(sip_lib, handle, t, value, kinds):
     assert sip_lib.sipFftSetPlanHint(handle, L.SIP_FFT_HINT_REAL_FUSED, value) == OK
     assert plan1d(sip_lib, handle, 1 << 20, t, F, 2) == OK
     assert [s["what"].split(" n=")[0] for s in describe(sip_lib, handle)["steps"]] == kinds
+
+
+def test_bluestein_limit(sip_lib, handle):
+    """Lengths above 2^27 are outside the API (the reference's limit); below
+    it every length plans, Bluestein's included."""
+    assert plan1d(sip_lib, handle, (1 << 27) + 1, C2C, F, 1) == INV
+    desc_ok = plan1d(sip_lib, handle, (1 << 27) - 1, C2C, F, 1)
+    assert desc_ok == OK
+    steps = describe(sip_lib, handle)["steps"]
+    assert steps[0]["m"] == 1 << 28

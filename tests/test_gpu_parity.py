@@ -175,3 +175,18 @@ def test_bluestein_lengths(cuda, n, batch, op, direction):
     out = gpu_run(cuda, op, direction, [n], batch, x)
     err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
     assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+
+
+@pytest.mark.parametrize("op,direction,n,batch", [(O.C2C, O.FORWARD, (1 << 22) + 1, 2),
+                                                   (O.C2C, O.INVERSE, 5000011, 1),
+                                                   (O.R2C, O.FORWARD, 2 * 4194319, 1)])
+def test_bluestein_above_2p22(cuda, op, direction, n, batch):
+    """Lengths with a large prime factor above 2^22: the convolution is longer
+    than the host's FP64 filter transform handles quickly, so its filter is
+    the library's own FP32 transform of the FP64-made sequence, on the GPU."""
+    from tests.fftcase import random_input
+
+    x = random_input(op, [n], batch, seed=n % 1000)
+    out = gpu_run(cuda, op, direction, [n], batch, x)
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, f"n={n}: rel_l2 {err:.3e}"
