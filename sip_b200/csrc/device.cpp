@@ -209,6 +209,7 @@ void prepare_device(FftPlan& plan) {
         plan.lanes = l;
     }
     for (Step& st : plan.steps) {
+        if (is_pair_kind(st.kind)) continue;  // no tables
         if (st.kind == StepKind::Blue) {
             st.chirp_buf = chirp_table(device, st.blue_n, st.blue_sign);
             st.blue.chirp = static_cast<const float2*>(st.chirp_buf->ptr);
@@ -314,6 +315,18 @@ void launch_one(const Step& st, cudaStream_t stream, const void* in, void* out, 
         check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
                         st.L.args.tw, stream),
               "tensor-core kernel launch");
+    } else if (is_pair_kind(st.kind)) {
+        PairPassArgs a = st.pair;
+        a.src = src;
+        a.dst = dst;
+        cudaError_t e = cudaSuccess;
+        switch (st.kind) {
+            case StepKind::PairPack: e = pair_pack(a, stream); break;
+            case StepKind::PairSeparate: e = pair_separate(a, stream); break;
+            case StepKind::PairCombine: e = pair_combine(a, stream); break;
+            default: e = pair_split(a, stream); break;
+        }
+        check(e, "pair pass launch");
     } else {
         RealPassArgs a = st.real;
         a.src = reinterpret_cast<const float2*>(src);

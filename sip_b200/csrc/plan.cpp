@@ -845,6 +845,51 @@ Step mirrored_step(const SkEntry* e, int n, int n_other, long long rows, const A
     return st;
 }
 
+// Odd real length above one tile whose complex FFT has a four-step split:
+// real rows 2p and 2p + 1 travel as complex row p (x_a + i x_b) through the
+// complex four-step of length n, between element-wise passes (R2C: pack, then
+// separate the two rows' bins from Z[k] and Z[n-k]; C2R: combine the two half
+// spectra into one complex spectrum, then split the real and imaginary
+// parts).  Four HBM round trips of the packed data instead of Bluestein's
+// convolution of twice the length.  Workspace: [0, zb) the packed rows
+// (pass B of the four-step writes back there), then the four-step scratch.
+// The reference takes such lengths whole into its arch35 real core
+// (core/fft/fftcore/fft_r2c_arch35.cpp:121-148).
+void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
+    const long long pairs = (rows + 1) / 2;
+    const size_t zb = ((size_t)(pairs * n * 8) + 255) / 256 * 256;
+    const long long h = n / 2 + 1;
+    Step first;
+    first.kind = r2c ? StepKind::PairPack : StepKind::PairCombine;
+    first.pair.n = n;
+    first.pair.rows = rows;
+    first.pair.in_pitch = r2c ? n : h;
+    first.pair.out_pitch = n;
+    first.pair.conj = (!r2c && plan.forward()) ? 1 : 0;
+    first.src = Loc::In;
+    first.dst = Loc::Ws;
+    first.what = std::string(r2c ? "r2c pair pack" : "c2r pair combine") + " n=" + std::to_string(n);
+    plan.steps.push_back(first);
+    C2COpts o;
+    o.sign = r2c ? -1 : 1;
+    o.src = Loc::Ws;
+    o.dst = Loc::Ws;
+    o.scratch_off = zb;
+    add_c2c_1d(plan, n, pairs, o);
+    Step last;
+    last.kind = r2c ? StepKind::PairSeparate : StepKind::PairSplit;
+    last.pair.n = n;
+    last.pair.rows = rows;
+    last.pair.in_pitch = n;
+    last.pair.out_pitch = r2c ? h : n;
+    last.pair.conj = (r2c && !plan.forward()) ? 1 : 0;
+    last.src = Loc::Ws;
+    last.dst = Loc::Out;
+    last.what = std::string(r2c ? "r2c pair separate" : "c2r pair split") + " n=" + std::to_string(n);
+    plan.steps.push_back(last);
+    plan.workspace_need = std::max(plan.workspace_need, zb + (size_t)(pairs * n * 8));
+}
+
 // Even real length whose half-length FFT M needs the four-step split.
 // Fused form (both mirrored kernels compiled for the split): R2C = column
 // pass A + row pass B with the post-process on mirrored row pairs; C2R =
@@ -1233,6 +1278,10 @@ void build_steps_inner(FftPlan& plan) {
             add_bluestein(plan, BLUE_C2C, n, b);
             return;
         }
+        if (!c2c && n % 2 == 1 && n > kMaxTileN && c2c_direct(n)) {
+            add_real_odd_large(plan, r2c, n, b);
+            return;
+        }
         if (!c2c && !real_direct(n)) {
             if (n % 2 == 0 && n / 2 <= kMaxBluesteinN)
                 add_real_bluestein_half(plan, r2c, n, b);
@@ -1357,6 +1406,8 @@ std::string describe(const FftPlan& plan) {
         } else if (st.kind == StepKind::Blue) {
             os << ",\"n\":" << st.blue.n << ",\"m\":" << st.blue.m << ",\"rows\":" << st.blue.rows
                << ",\"post\":" << (st.blue_post ? "true" : "false");
+        } else if (is_pair_kind(st.kind)) {
+            os << ",\"n\":" << st.pair.n << ",\"rows\":" << st.pair.rows << ",\"conj\":" << st.pair.conj;
         } else {
             os << ",\"m\":" << st.real.m << ",\"rows\":" << st.real.rows << ",\"conj\":" << st.real.conj;
         }

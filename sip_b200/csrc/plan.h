@@ -42,12 +42,26 @@ using BufPtr = std::shared_ptr<DeviceBuf>;
 // Operand of a step.
 enum class Loc : int { In = 0, Out = 1, Ws = 2 };
 
-enum class StepKind : int { Tile = 0, RealPost = 1, RealPre = 2, Tc = 3, Blue = 4 };
+enum class StepKind : int {
+    Tile = 0,
+    RealPost = 1,
+    RealPre = 2,
+    Tc = 3,
+    Blue = 4,
+    // element-wise passes of odd real lengths above one tile (real_kernels.h)
+    PairPack = 5,
+    PairSeparate = 6,
+    PairCombine = 7,
+    PairSplit = 8,
+};
+
+inline bool is_pair_kind(StepKind k) { return k >= StepKind::PairPack && k <= StepKind::PairSplit; }
 
 struct Step {
     StepKind kind = StepKind::Tile;
     TileLaunch L;
     RealPassArgs real{};  // RealPost / RealPre
+    PairPassArgs pair{};  // PairPack / PairSeparate / PairCombine / PairSplit
     Loc src = Loc::In, dst = Loc::Out;
     size_t src_off = 0, dst_off = 0;  // byte offsets into the operand
     // Which tile index the plan's batch runs along (for executing fewer rows

@@ -79,4 +79,42 @@ SIP_HD void real_pre_pair(const float2* x, long long k, long long m, const float
     *zmk = make_float2(e.x + od.y, -e.y + od.x);
 }
 
+// ---------------------------------------- odd real lengths above one tile
+// Two real rows travel as one complex row z = x_a + i x_b of length n
+// (the two-rows-per-transform packing of tile_io.cuh load_r2c_pair /
+// store_r2c_pair, applied to whole rows around the complex four-step).
+
+// Bin k <= n/2 of rows a and b from Z = FFT(z): (Z[k] + conj Z[n-k]) / 2 and
+// (Z[k] - conj Z[n-k]) / 2i, conjugated for the inverse direction.
+SIP_HD void pair_separate_elem(const float2* z, long long k, long long n, bool conj, float2* xa, float2* xb) {
+    const float2 zk = SIP_LDG(z + k), zm = SIP_LDG(z + (k == 0 ? 0 : n - k));
+    float2 a = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    float2 b = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    if (conj) {
+        a.y = -a.y;
+        b.y = -b.y;
+    }
+    *xa = a;
+    *xb = b;
+}
+
+// Z[k], k < n, of the complex row that carries the spectra of rows a and b
+// (half spectra of n/2 + 1 bins; xb null: a zero row): Xa[k] + i Xb[k] with
+// the Hermitian halves, the DC bin's imaginary parts ignored; `fwd`
+// (C2R forward, hfft) conjugates the input spectra.
+SIP_HD float2 pair_combine_elem(const float2* xa, const float2* xb, long long k, long long n, bool fwd) {
+    const long long kk = 2 * k <= n ? k : n - k;
+    float2 a = SIP_LDG(xa + kk);
+    float2 b = xb != nullptr ? SIP_LDG(xb + kk) : make_float2(0.f, 0.f);
+    if (kk == 0) {
+        a.y = 0.f;
+        b.y = 0.f;
+    }
+    if ((2 * k > n) != fwd) {
+        a.y = -a.y;
+        b.y = -b.y;
+    }
+    return make_float2(a.x - b.y, a.y + b.x);
+}
+
 }  // namespace sipfft

@@ -46,15 +46,15 @@
        process fused (4); small CTAs (2-4 warps) leave more of them per SM.  \
        The second entry of a length is a hint variant. */                    \
     X(0, 500, 2, 64, OP_R2C_HALF, SK_ROWS, -1, false, 2, 8, 15, 25, 5, 4)            \
-    X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 5, 10, 10)           \
+    X(1, 500, 4, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 11, 20, 25)              \
     X(2, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 15, 25, 15, 8)         \
-    X(3, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 15, 15, 8, 25)          \
+    X(3, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 11, 25, 8, 15)          \
     X(7, 3000, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 9, 25, 8, 15)           \
     X(4, 3000, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 7, 15, 25, 8)          \
     X(5, 3000, 2, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 1, 25, 8, 15)           \
     /* real rows of N = 2048, 4096, 8192 (half lengths 1024, 2048, 4096) */  \
     X(6, 1024, 4, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 15, 16, 16, 4)         \
-    X(7, 1024, 4, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 9, 4, 16, 16)           \
+    X(7, 1024, 4, 256, OP_C2R_HALF, SK_ROWS, 1, false, 2, 2, 11, 16, 16, 4)          \
     X(0, 2048, 1, 128, OP_R2C_HALF, SK_ROWS, -1, false, 2, 4, 15, 16, 16, 8)         \
     X(1, 2048, 1, 128, OP_C2R_HALF, SK_ROWS, 1, false, 2, 4, 15, 8, 16, 16)          \
     X(2, 4096, 1, 256, OP_R2C_HALF, SK_ROWS, -1, false, 2, 2, 15, 16, 32, 8)         \
@@ -72,6 +72,7 @@
        shape from a run-time compiled sweep: 4 % faster than 2 x 192) */     \
     X(7, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 15, 27, 9, 9)          \
     X(0, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 9, 27, 9, 9)            \
+    X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 11, 27, 9, 9)           \
     X(1, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 1, 27, 9, 9)           \
     X(2, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 1, 27, 9, 9)            \
     /* real 2^20 fused four-step: R2C pass B + post, C2R pre + pass A        \

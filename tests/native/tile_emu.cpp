@@ -364,6 +364,41 @@ void emu_blue_step(const Step& st, const void* src, void* dst) {
     }
 }
 
+// Element-wise passes of odd real lengths above one tile (real_kernels.cu).
+void emu_pair_step(const Step& st, const void* src, void* dst) {
+    const PairPassArgs& a = st.pair;
+    const long long pairs = (a.rows + 1) / 2;
+    for (long long p = 0; p < pairs; ++p) {
+        const bool second = 2 * p + 1 < a.rows;
+        if (st.kind == StepKind::PairPack) {
+            const float* xa = static_cast<const float*>(src) + 2 * p * a.in_pitch;
+            float2* z = static_cast<float2*>(dst) + p * a.out_pitch;
+            for (long long j = 0; j < a.n; ++j) z[j] = make_float2(xa[j], second ? xa[a.in_pitch + j] : 0.f);
+        } else if (st.kind == StepKind::PairSeparate) {
+            const float2* z = static_cast<const float2*>(src) + p * a.in_pitch;
+            float2* outa = static_cast<float2*>(dst) + 2 * p * a.out_pitch;
+            for (long long k = 0; 2 * k <= a.n; ++k) {
+                float2 xa, xb;
+                pair_separate_elem(z, k, a.n, a.conj != 0, &xa, &xb);
+                outa[k] = xa;
+                if (second) outa[a.out_pitch + k] = xb;
+            }
+        } else if (st.kind == StepKind::PairCombine) {
+            const float2* xa = static_cast<const float2*>(src) + 2 * p * a.in_pitch;
+            float2* z = static_cast<float2*>(dst) + p * a.out_pitch;
+            for (long long k = 0; k < a.n; ++k)
+                z[k] = pair_combine_elem(xa, second ? xa + a.in_pitch : nullptr, k, a.n, a.conj != 0);
+        } else {
+            const float2* z = static_cast<const float2*>(src) + p * a.in_pitch;
+            float* outa = static_cast<float*>(dst) + 2 * p * a.out_pitch;
+            for (long long j = 0; j < a.n; ++j) {
+                outa[j] = z[j].x;
+                if (second) outa[a.out_pitch + j] = z[j].y;
+            }
+        }
+    }
+}
+
 void emu_real_step(const Step& st, const void* src, void* dst) {
     std::vector<float2> tw = tw2_host(st);
     const RealPassArgs& r = st.real;
@@ -495,6 +530,7 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
                 stc.L.args.mul = filt.data();
             }
             if (st.kind == StepKind::Blue) emu_blue_step(st, s, d);
+            else if (is_pair_kind(st.kind)) emu_pair_step(st, s, d);
             else if (st.kind == StepKind::Tile) emu_tile_step(stc, s, d);
             else if (st.kind == StepKind::Tc) emu_tc_step(st, s, d);
             else emu_real_step(stc, s, d);

@@ -190,3 +190,18 @@ def test_bluestein_above_2p22(cuda, op, direction, n, batch):
     out = gpu_run(cuda, op, direction, [n], batch, x)
     err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
     assert err <= REL_L2_TOL, f"n={n}: rel_l2 {err:.3e}"
+
+
+@pytest.mark.parametrize("n", [59049, 98415, 177147])
+@pytest.mark.parametrize("op,direction", [(O.R2C, O.FORWARD), (O.R2C, O.INVERSE), (O.C2R, O.INVERSE),
+                                          (O.C2R, O.FORWARD)])
+@pytest.mark.parametrize("batch", [1, 6, 7])
+def test_odd_real_above_one_tile(cuda, n, op, direction, batch):
+    """Odd real lengths above one tile (3^10, 3^9 5, 3^11): row pairs through
+    the complex four-step, as the reference's arch35 real core takes them."""
+    from tests.fftcase import random_input
+
+    x = random_input(op, [n], batch, seed=n + batch)
+    out = gpu_run(cuda, op, direction, [n], batch, x)
+    err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
+    assert err <= REL_L2_TOL, f"n={n} batch={batch}: rel_l2 {err:.3e}"
