@@ -448,7 +448,8 @@ def serving(torch, count: int, budget_gb: float = 16.0) -> dict:
         return cb
 
     out = {"requests": count, "budget_gb": budget_gb, "plain_plan_cache": 10,
-           "sample": f"{count} requests of the 100k-request stream (seed 20261203)"}
+           "sample": f"{count} requests of the 100k-request stream (seed 20261203), each run",
+           "filter": "conj spectrum of the chirp, made once per length by the library's own C2C on the GPU"}
     warm = make_requests(64, rate_hz=float("inf"), seed=1)
     Scheduler(queue, budget).run(warm)
     Scheduler(plain, budget, max_inflight=64, max_group=1).run(make_requests(64, rate_hz=float("inf"), seed=1))
@@ -796,7 +797,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32 vs tensor-core comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-form comparison")
     ap.add_argument("--no-other", action="store_true", help="skip the 1D/2D/3D C2C configurations")
-    ap.add_argument("--serve-requests", type=int, default=3000, help="requests per serving run")
+    ap.add_argument("--serve-requests", type=int, default=30000, help="requests per serving run")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="CPU baseline seconds per size")
     ap.add_argument("--ref-seconds", type=float, default=1.5, help="reference arm seconds per size per step")
     args = ap.parse_args()

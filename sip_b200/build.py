@@ -42,6 +42,7 @@ UNITS = [
     ("bluestein.cu", [], "bluestein.o"),
     ("bluestein_host.cpp", [], "bluestein_host.o"),
     ("real_kernels.cu", [], "real_kernels.o"),
+    ("cluster.cu", [], "cluster.o"),
     ("plan.cpp", [], "plan.o"),
     ("device.cpp", [], "device.o"),
     ("api.cpp", [], "api.o"),

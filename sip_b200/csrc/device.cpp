@@ -210,6 +210,16 @@ void prepare_device(FftPlan& plan) {
     }
     for (Step& st : plan.steps) {
         if (is_pair_kind(st.kind)) continue;  // no tables
+        if (st.kind == StepKind::Cluster) {
+            st.tw = basis_table(device, st.host_plan, st.radices);
+            st.tw_b = basis_table(device, st.cl_plan_b, st.cl_radices_b);
+            st.tw2 = split_table(device, st.tw2_n, st.cl_b.tw4_shift);
+            st.L.args.tw = static_cast<const float2*>(st.tw->ptr);
+            st.cl_b.tw = static_cast<const float2*>(st.tw_b->ptr);
+            st.cl_b.tw2 = static_cast<const float2*>(st.tw2->ptr);
+            check(cluster_prepare(st.cl), "cluster_prepare");
+            continue;
+        }
         if (st.kind == StepKind::Blue) {
             st.chirp_buf = chirp_table(device, st.blue_n, st.blue_sign);
             st.blue.chirp = static_cast<const float2*>(st.chirp_buf->ptr);
@@ -315,6 +325,11 @@ void launch_one(const Step& st, cudaStream_t stream, const void* in, void* out, 
         check(tc_launch(st.tc_fn, st.L.grid, st.L.args, src, dst, static_cast<const uint16_t*>(st.tc_bmat->ptr),
                         st.L.args.tw, stream),
               "tensor-core kernel launch");
+    } else if (st.kind == StepKind::Cluster) {
+        TileArgs a = st.L.args, b = st.cl_b;
+        a.src = src;
+        b.dst = dst;
+        check(cluster_launch(st.cl, st.cl_transforms, a, b, stream), "cluster kernel launch");
     } else if (is_pair_kind(st.kind)) {
         PairPassArgs a = st.pair;
         a.src = src;

@@ -353,8 +353,70 @@ struct C2COpts {
     size_t scratch_off = 0;  // four-step scratch region in the workspace
 };
 
+// The cluster four-step (cluster.h) for a plain C2C of few transforms: one
+// cluster of CTAs per transform, so that small batches fill the GPU (C2C
+// 4096 x 256: 1024 CTAs instead of 256).  Used when a configuration is
+// compiled for the length and the batch holds at most 2^21 points;
+// SIP_FFT_CLUSTER=0 disables it, =1 uses it for any batch.
+const ClEntry* pick_cluster(long long n, long long batch, int sign, const C2COpts& o) {
+    if (o.src != Loc::In || o.dst != Loc::Out || o.src_off || o.dst_off || o.last_flags) return nullptr;
+    if (g_hint_generic || std::getenv("SIP_FFT_GENERIC_ONLY")) return nullptr;
+    const char* e = std::getenv("SIP_FFT_CLUSTER");
+    const int mode = (e != nullptr && *e) ? std::atoi(e) : -1;
+    if (mode == 0) return nullptr;
+    if (mode != 1 && batch * n > (1LL << 21)) return nullptr;
+    return cluster_find((int)n, sign);
+}
+
+void add_cluster_c2c(FftPlan& plan, const ClEntry* ce, long long n, long long batch) {
+    Step st;
+    st.kind = StepKind::Cluster;
+    st.cl = ce;
+    st.cl_transforms = batch;
+    int tw_entries = 0;
+    st.radices = ce->ra;
+    st.host_plan = make_plandev(ce->n1, ce->ra, &tw_entries);
+    st.cl_radices_b = ce->rb;
+    st.cl_plan_b = make_plandev(ce->n2, ce->rb, &tw_entries);
+    int shift = 0;
+    while ((1LL << (2 * shift)) < n) ++shift;
+    TileArgs& a = st.L.args;  // columns i2 of x viewed as [n1][n2]
+    a.N = ce->n1;
+    a.P = ce->pa;
+    a.inner = ce->n2;
+    a.in_odist = n;
+    a.in_idist = 1;
+    a.in_stride = ce->n2;
+    a.scale = 1.0f;
+    a.tw4_shift = shift;
+    TileArgs& b = st.cl_b;  // rows k1 of Y, X[k1 + n1 k2] out
+    b.N = ce->n2;
+    b.P = ce->pb;
+    b.inner = ce->n1;
+    b.out_odist = n;
+    b.out_idist = 1;
+    b.out_stride = ce->n1;
+    b.scale = 1.0f;
+    b.tw4_shift = shift;
+    st.tw2_kind = 2;  // the cross twiddles W_n^m, pass B's gather
+    st.tw2_n = n;
+    st.tw2_count = (1LL << shift) + (n + (1LL << shift) - 1) / (1LL << shift);
+    st.L.sign = ce->sign;
+    st.L.block = ce->T;
+    st.L.smem_bytes = ce->smem;
+    st.L.grid = (int)(batch * ce->C);
+    st.src = Loc::In;
+    st.dst = Loc::Out;
+    st.what = "c2c cluster n=" + std::to_string(n) + " [" + std::to_string(ce->C) + " CTAs per transform]";
+    plan.steps.push_back(st);
+}
+
 void add_c2c_1d(FftPlan& plan, long long n, long long batch, const C2COpts& o) {
     const int sign = o.sign != 0 ? o.sign : c2c_sign(plan);
+    if (const ClEntry* ce = n <= kMaxTileN ? pick_cluster(n, batch, sign, o) : nullptr) {
+        add_cluster_c2c(plan, ce, n, batch);
+        return;
+    }
     if (n <= kMaxTileN) {
         AxisIO io;
         io.inner = batch;
@@ -1408,6 +1470,9 @@ std::string describe(const FftPlan& plan) {
                << ",\"post\":" << (st.blue_post ? "true" : "false");
         } else if (is_pair_kind(st.kind)) {
             os << ",\"n\":" << st.pair.n << ",\"rows\":" << st.pair.rows << ",\"conj\":" << st.pair.conj;
+        } else if (st.kind == StepKind::Cluster) {
+            os << ",\"n\":" << st.cl->n << ",\"cluster\":" << st.cl->C << ",\"threads\":" << st.cl->T
+               << ",\"transforms\":" << st.cl_transforms << ",\"sign\":" << st.cl->sign;
         } else {
             os << ",\"m\":" << st.real.m << ",\"rows\":" << st.real.rows << ",\"conj\":" << st.real.conj;
         }

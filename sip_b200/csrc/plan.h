@@ -17,6 +17,7 @@
 
 #include "fft_api.h"
 #include "bluestein.h"
+#include "cluster.h"
 #include "real_kernels.h"
 #include "sk_registry.h"
 #include "tile_launch.h"
@@ -53,6 +54,8 @@ enum class StepKind : int {
     PairSeparate = 6,
     PairCombine = 7,
     PairSplit = 8,
+    // one C2C transform per thread-block cluster (cluster.h)
+    Cluster = 9,
 };
 
 inline bool is_pair_kind(StepKind k) { return k >= StepKind::PairPack && k <= StepKind::PairSplit; }
@@ -62,6 +65,15 @@ struct Step {
     TileLaunch L;
     RealPassArgs real{};  // RealPost / RealPre
     PairPassArgs pair{};  // PairPack / PairSeparate / PairCombine / PairSplit
+    // Cluster: L.args drives pass A (n1-point columns), cl_b pass B (n2-point
+    // rows, the cross twiddle table in its tw2); cl_plan_b / cl_radices_b
+    // describe pass B's radix passes; cl_transforms transforms per exec.
+    const ClEntry* cl = nullptr;
+    TileArgs cl_b{};
+    PlanDev cl_plan_b{};
+    std::vector<int> cl_radices_b;
+    long long cl_transforms = 0;
+    BufPtr tw_b;
     Loc src = Loc::In, dst = Loc::Out;
     size_t src_off = 0, dst_off = 0;  // byte offsets into the operand
     // Which tile index the plan's batch runs along (for executing fewer rows

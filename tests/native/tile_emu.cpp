@@ -22,6 +22,7 @@
 #include "real_math.cuh"
 #include "sk_configs.h"
 #include "sk_kernel.cuh"
+#include "cluster_configs.h"
 #include "tc_core.cuh"
 
 using namespace sipfft;
@@ -178,6 +179,77 @@ void emu_sk_run(const TileArgs& a) {
 
 using EmuSkFn = void (*)(const TileArgs&);
 
+// ---- cluster four-step: the kernel's phases rank by rank, the cluster's
+// shared memories as host vectors
+template <class CC, int PASS>
+void emu_cl_passes_a(const TileArgs& a, const TileCtx& c, float2* buf, float2* rows) {
+    using SP = SkPass<typename CC::KA, PASS>;
+    std::vector<typename SP::Regs> regs(CC::T);
+    for (int tid = 0; tid < CC::T; ++tid) SP::read(tid, a, c, buf, regs[tid]);
+    if constexpr (SP::LAST) {
+        for (int tid = 0; tid < CC::T; ++tid) cl_pass_a_write_rows<CC, PASS>(tid, rows, regs[tid]);
+    } else {
+        for (int tid = 0; tid < CC::T; ++tid) SP::write_smem(tid, buf, regs[tid]);
+        emu_cl_passes_a<CC, PASS + 1>(a, c, buf, rows);
+    }
+}
+
+template <class CC>
+void emu_cluster_run(const TileArgs& a, const TileArgs& b, long long transforms) {
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    for (long long tr = 0; tr < transforms; ++tr) {
+        std::vector<std::vector<float2>> rows(CC::C, std::vector<float2>(CC::N1 * CC::PA, make_float2(nan, nan)));
+        for (int r = 0; r < CC::C; ++r) {
+            std::vector<float2> abuf(CC::KA::BUF, make_float2(nan, nan));
+            TileCtx ca;
+            ca.i0 = r * CC::PA;
+            ca.cnt = CC::PA;
+            ca.in_base = tr * CC::N + ca.i0;
+            ca.out_base = 0;
+            for (int tid = 0; tid < CC::T; ++tid) sk_stage<typename CC::KA>(tid, a, ca, abuf.data());
+            emu_cl_passes_a<CC, 0>(a, ca, abuf.data(), rows[r].data());
+        }
+        for (int r = 0; r < CC::C; ++r) {
+            std::vector<float2> bbuf(CC::KB::BUF, make_float2(nan, nan));
+            for (int tid = 0; tid < CC::T; ++tid)
+                cl_gather<CC>(tid, b, r, [&](int p) -> const float2* { return rows[p].data(); }, bbuf.data());
+            TileCtx cb;
+            cb.i0 = r * CC::PB;
+            cb.cnt = CC::PB;
+            cb.in_base = 0;
+            cb.out_base = tr * CC::N + cb.i0;
+            emu_sk_passes<typename CC::KB, 0>(b, cb, bbuf.data());
+        }
+    }
+}
+
+using EmuClFn = void (*)(const TileArgs&, const TileArgs&, long long);
+
+template <class K>
+std::vector<int> emu_radices_of() {
+    std::vector<int> r;
+    for (int p = 0; p < K::NP; ++p) r.push_back(K::radix(p));
+    return r;
+}
+
+template <class CC>
+ClEntry emu_cl_entry() {
+    ClEntry e;
+    e.n = CC::N;
+    e.n1 = CC::N1;
+    e.n2 = CC::N2;
+    e.C = CC::C;
+    e.T = CC::T;
+    e.sign = CC::SIGN;
+    e.pa = CC::PA;
+    e.pb = CC::PB;
+    e.ra = emu_radices_of<typename CC::KA>();
+    e.rb = emu_radices_of<typename CC::KB>();
+    e.smem = CC::SMEM_VALUES * 8;
+    e.fn = reinterpret_cast<const void*>(&emu_cluster_run<CC>);
+    return e;
+}
+
 template <class K, int STAGES>
 SkEntry emu_entry(std::vector<int> radices) {
     SkEntry e;
@@ -229,6 +301,18 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant)
         if (variant-- == 0) return &e;
     }
     return first;
+}
+const ClEntry* cluster_find(int n, int sign) {
+    static const std::vector<ClEntry> reg = [] {
+        std::vector<ClEntry> v;
+#define SIP_EMU_CL(CC) v.push_back(emu_cl_entry<CC>());
+        SIP_CL_CONFIGS(SIP_EMU_CL)
+#undef SIP_EMU_CL
+        return v;
+    }();
+    for (const ClEntry& e : reg)
+        if (e.n == n && e.sign == sign) return &e;
+    return nullptr;
 }
 // The harness runs only the kernels it instantiates: no run-time compiled ones.
 const SkEntry* sk_jit_entry(int, int, int, bool, int, long long, bool) { return nullptr; }
@@ -362,6 +446,18 @@ void emu_blue_step(const Step& st, const void* src, void* dst) {
         for (long long row = 0; row < a.rows; ++row)
             for (long long k = 0; k < cnt; ++k) blue_post_elem(a, row, k);
     }
+}
+
+// Cluster four-step step: the harness's runner of the step's configuration.
+void emu_cluster_step(const Step& st, const void* src, void* dst) {
+    TileArgs a = st.L.args, b = st.cl_b;
+    std::vector<float2> twa = basis_host(st.radices), twb = basis_host(st.cl_radices_b), tw2 = tw2_host(st);
+    a.src = src;
+    a.tw = twa.data();
+    b.dst = dst;
+    b.tw = twb.data();
+    b.tw2 = tw2.data();
+    reinterpret_cast<EmuClFn>(const_cast<void*>(st.cl->fn))(a, b, st.cl_transforms);
 }
 
 // Element-wise passes of odd real lengths above one tile (real_kernels.cu).
@@ -531,6 +627,7 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
             }
             if (st.kind == StepKind::Blue) emu_blue_step(st, s, d);
             else if (is_pair_kind(st.kind)) emu_pair_step(st, s, d);
+            else if (st.kind == StepKind::Cluster) emu_cluster_step(st, s, d);
             else if (st.kind == StepKind::Tile) emu_tile_step(stc, s, d);
             else if (st.kind == StepKind::Tc) emu_tc_step(st, s, d);
             else emu_real_step(stc, s, d);

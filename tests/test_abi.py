@@ -226,7 +226,8 @@ def test_partial_overlap_rejected(sip_lib, handle):
 
 
 @pytest.mark.parametrize("t,sizes,kinds", [
-    (C2C, [4096], ["c2c rows"]),
+    (C2C, [4096], ["c2c cluster"]),   # two transforms: one thread-block cluster each
+    (C2C, [6000], ["c2c rows"]),
     (C2C, [65536], ["four-step A", "four-step B"]),
     (C2C, [2048, 2048], ["c2c axis 1", "c2c axis 0"]),
     (C2C, [256, 256, 256], ["c2c axis 2", "c2c axis 1", "c2c axis 0"]),
@@ -262,7 +263,7 @@ def test_compute_mode(sip_lib, handle):
 
 def test_plan_trace_env():
     code = ("import ctypes,sys; sys.path.insert(0, %r); from sip_b200 import _lib as L; l=L.lib(); "
-            "h=ctypes.c_void_p(); l.asdFftCreate(ctypes.byref(h)); l.asdFftMakePlan1D(h, 4096, 0x10, 0x10, 2, 0x10)"
+            "h=ctypes.c_void_p(); l.asdFftCreate(ctypes.byref(h)); l.asdFftMakePlan1D(h, 4096, 0x10, 0x10, 1024, 0x10)"
             % str(ROOT))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                        env={**os.environ, "ASDSIP_FFT_PLAN_TRACE": "1"})
@@ -292,9 +293,9 @@ def test_generic_hint_large_real_uses_queueable_passes(sip_lib, handle):
 
 def test_tune_cache_env(tmp_path):
     cache = tmp_path / "tune.txt"
-    cache.write_text("# type dir dims batch P E generic order\n16 16 4096 64 1 32 1 0\n")
+    cache.write_text("# type dir dims batch P E generic order\n16 16 4096 1024 1 32 1 0\n")
     code = ("import ctypes,sys,json; sys.path.insert(0, %r); from sip_b200.fft import FftHandle; "
-            "h=FftHandle(); h.make_plan_1d(4096, 0x10, 0x10, 64); s=h.describe()['steps'][0]; "
+            "h=FftHandle(); h.make_plan_1d(4096, 0x10, 0x10, 1024); s=h.describe()['steps'][0]; "
             "print(json.dumps([s['sk'], s['e'], s['P']]))" % str(ROOT))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                        env={**os.environ, "SIP_FFT_TUNE_CACHE": str(cache)})

@@ -19,40 +19,47 @@ pytestmark = pytest.mark.gpu
 REL_L2_TOL = 1e-6
 
 
-def _check(torch, op, direction, sizes, batch):
+def _check(torch, op, direction, sizes, batch, record=None):
     ishape, idt, _, _ = shapes(op, sizes, batch)
     x = O.ut_input(ishape, idt)
     out = gpu_run(torch, op, direction, sizes, batch, x)
     gold = O.golden(op, direction, x, sizes)
     bad = O.ref_check_mismatches(out, gold)
+    # the bins that meet the reference's isclose(1e-3, 1e-5) only with the
+    # absolute tolerance floored at 1e-6 of the peak (near-zero bins of long
+    # FP32 transforms): recorded per case (junit property
+    # "isclose_floor_bins") and named in the failure message
+    strict = O.isclose_mismatches(out, gold, 1e-3, 1e-5)
+    if record is not None:
+        record("isclose_floor_bins", strict - bad)
     err = O.rel_l2(out, O.fp64(op, direction, x, sizes))
     assert bad == 0, f"{bad} elements outside isclose(1e-3, 1e-5); rel_l2={err:.3e}"
-    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}"
+    assert err <= REL_L2_TOL, f"rel_l2 vs FP64 {err:.3e}; {strict} bins needed the floored atol"
 
 
 @pytest.mark.parametrize("batch,n,direction", RC.C2C_1D)
-def test_ref_c2c_1d(cuda, batch, n, direction):
-    _check(cuda, O.C2C, direction, [n], batch)
+def test_ref_c2c_1d(cuda, record_property, batch, n, direction):
+    _check(cuda, O.C2C, direction, [n], batch, record_property)
 
 
 @pytest.mark.parametrize("batch,n,direction", RC.R2C_1D)
-def test_ref_r2c_1d(cuda, batch, n, direction):
-    _check(cuda, O.R2C, direction, [n], batch)
+def test_ref_r2c_1d(cuda, record_property, batch, n, direction):
+    _check(cuda, O.R2C, direction, [n], batch, record_property)
 
 
 @pytest.mark.parametrize("batch,n,direction", RC.C2R_1D)
-def test_ref_c2r_1d(cuda, batch, n, direction):
-    _check(cuda, O.C2R, direction, [n], batch)
+def test_ref_c2r_1d(cuda, record_property, batch, n, direction):
+    _check(cuda, O.C2R, direction, [n], batch, record_property)
 
 
 @pytest.mark.parametrize("x,y,batch,direction", RC.C2C_2D)
-def test_ref_c2c_2d(cuda, x, y, batch, direction):
-    _check(cuda, O.C2C, direction, [x, y], batch)
+def test_ref_c2c_2d(cuda, record_property, x, y, batch, direction):
+    _check(cuda, O.C2C, direction, [x, y], batch, record_property)
 
 
 @pytest.mark.parametrize("x,y,z,batch,direction", RC.C2C_3D)
-def test_ref_c2c_3d(cuda, x, y, z, batch, direction):
-    _check(cuda, O.C2C, direction, [x, y, z], batch)
+def test_ref_c2c_3d(cuda, record_property, x, y, z, batch, direction):
+    _check(cuda, O.C2C, direction, [x, y, z], batch, record_property)
 
 
 # Real multi-dimensional transforms (R2C/C2R along the last axis, C2C on the others).
@@ -205,3 +212,26 @@ def test_odd_real_above_one_tile(cuda, n, op, direction, batch):
     out = gpu_run(cuda, op, direction, [n], batch, x)
     err = O.rel_l2(out, O.fp64(op, direction, x, [n]))
     assert err <= REL_L2_TOL, f"n={n} batch={batch}: rel_l2 {err:.3e}"
+
+
+@pytest.mark.parametrize("n,batch", [(1024, 1024), (4096, 256), (8192, 3), (4096, 1)])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_cluster_four_step(cuda, n, batch, direction, monkeypatch):
+    """Small C2C batches run one transform per thread-block cluster (the
+    CTAs exchanging through distributed shared memory); the same plan with
+    the cluster form switched off runs the one-CTA-per-transform kernel.
+    Both match FP64."""
+    from tests.fftcase import random_input
+    from sip_b200.fft import FftHandle
+
+    x = random_input(O.C2C, [n], batch, seed=n + batch)
+    h = FftHandle()
+    assert h.make_plan_1d(n, O.C2C, direction, batch) == 0
+    assert h.describe()["steps"][0]["kind"] == 9   # the cluster step
+    h.destroy()
+    want = O.fp64(O.C2C, direction, x, [n])
+    out = gpu_run(cuda, O.C2C, direction, [n], batch, x)
+    assert O.rel_l2(out, want) <= REL_L2_TOL
+    monkeypatch.setenv("SIP_FFT_CLUSTER", "0")
+    out0 = gpu_run(cuda, O.C2C, direction, [n], batch, x)
+    assert O.rel_l2(out0, want) <= REL_L2_TOL
