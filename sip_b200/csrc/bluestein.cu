@@ -1,5 +1,8 @@
-// Bluestein pre/post passes and the chirp table (bluestein.cuh).
+// Bluestein pre/post passes and the chirp table (bluestein.cuh).  The pre
+// and post passes launch with programmatic dependent launch (launch_attr.h).
 #include "bluestein.h"
+
+#include "launch_attr.h"
 
 namespace sipfft {
 
@@ -8,6 +11,8 @@ namespace {
 constexpr int kBlueBlock = 256;
 
 __global__ void k_blue_pre(const BluesteinArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     float2* dst = static_cast<float2*>(a.dst);
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y)
         for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < a.m;
@@ -16,6 +21,8 @@ __global__ void k_blue_pre(const BluesteinArgs a) {
 }
 
 __global__ void k_blue_post(const BluesteinArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long cnt = blue_out_count(a);
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y)
         for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cnt;
@@ -68,13 +75,11 @@ cudaError_t bluestein_prepare() {
 }
 
 cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream) {
-    k_blue_pre<<<grid2(a.m, a.rows), kBlueBlock, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_blue_pre, grid2(a.m, a.rows), dim3(kBlueBlock), 0, stream, a);
 }
 
 cudaError_t bluestein_post(const BluesteinArgs& a, cudaStream_t stream) {
-    k_blue_post<<<grid2(blue_out_count(a), a.rows), kBlueBlock, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_blue_post, grid2(blue_out_count(a), a.rows), dim3(kBlueBlock), 0, stream, a);
 }
 
 cudaError_t gen_blue_b(float2* out, long long n, long long m, int sign, cudaStream_t stream) {

@@ -42,6 +42,25 @@ typedef unsigned long long uintptr_t;
 
 namespace sipfft {
 
+// ------------------------------------------- programmatic dependent launch
+// A kernel launched with the programmatic-stream-serialization attribute
+// (launch_attr.h) may start while the previous kernel of its stream still
+// runs.  grid_dep_wait() returns once that kernel has completed and its
+// memory operations are visible, so every such kernel calls it before its
+// first global-memory access.  grid_dep_launch() lets the stream's next
+// kernel of that kind start launching; it waits in turn.  Both do nothing
+// in a kernel launched without the attribute, and on the host.
+SIP_HD void grid_dep_wait() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+#endif
+}
+SIP_HD void grid_dep_launch() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+#endif
+}
+
 // ---------------------------------------------------------------- complex
 SIP_HD float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 SIP_HD float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }

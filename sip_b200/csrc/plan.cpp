@@ -354,17 +354,18 @@ struct C2COpts {
 };
 
 // The cluster four-step (cluster.h) for a plain C2C of few transforms: one
-// cluster of CTAs per transform, so that small batches fill the GPU (C2C
-// 4096 x 256: 1024 CTAs instead of 256).  Used when a configuration is
-// compiled for the length and the batch holds at most 2^21 points;
-// SIP_FFT_CLUSTER=0 disables it, =1 uses it for any batch.
+// cluster of CTAs per transform (C2C 4096 x 256: 1024 CTAs instead of 256).
+// Opt-in (SIP_FFT_CLUSTER=1) for the lengths with a compiled configuration:
+// on B200 it was 15-80 % slower than one CTA per transform at every batch
+// measured (4096 x 64 .. 512, 1024 x 1024 / 2048, 8192 x 128 / 256), the
+// cluster launch, the two cluster barriers and the DSMEM gather costing more
+// than the wider spread of the loads gains.
 const ClEntry* pick_cluster(long long n, long long batch, int sign, const C2COpts& o) {
+    (void)batch;
     if (o.src != Loc::In || o.dst != Loc::Out || o.src_off || o.dst_off || o.last_flags) return nullptr;
     if (g_hint_generic || std::getenv("SIP_FFT_GENERIC_ONLY")) return nullptr;
     const char* e = std::getenv("SIP_FFT_CLUSTER");
-    const int mode = (e != nullptr && *e) ? std::atoi(e) : -1;
-    if (mode == 0) return nullptr;
-    if (mode != 1 && batch * n > (1LL << 21)) return nullptr;
+    if (e == nullptr || std::atoi(e) != 1) return nullptr;
     return cluster_find((int)n, sign);
 }
 

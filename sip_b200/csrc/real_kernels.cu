@@ -1,6 +1,10 @@
 // Real-transform pre/post passes for lengths beyond one tile (element
-// formulas in real_math.cuh).
+// formulas in real_math.cuh).  Launched with programmatic dependent launch
+// (launch_attr.h): each kernel waits for the previous one before its first
+// global-memory access.
 #include "real_kernels.h"
+
+#include "launch_attr.h"
 
 #include "real_math.cuh"
 
@@ -11,6 +15,8 @@ namespace {
 // One thread per pair (k, m - k), k in [0, m/2]: each value and each
 // twiddle is read once (the mirror's twiddle follows from W_{2m}^k).
 __global__ void k_real_post(const RealPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = a.m / 2 + 1;
     const bool cj = a.conj != 0;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
@@ -30,6 +36,8 @@ __global__ void k_real_post(const RealPassArgs a) {
 }
 
 __global__ void k_real_pre(const RealPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = a.m / 2 + 1;
     const bool cj = a.conj != 0;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
@@ -49,6 +57,8 @@ __global__ void k_real_pre(const RealPassArgs a) {
 }
 
 __global__ void k_pair_pack(const PairPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = (a.rows + 1) / 2;
     for (long long p = blockIdx.y; p < pairs; p += gridDim.y) {
         const float* xa = static_cast<const float*>(a.src) + 2 * p * a.in_pitch;
@@ -61,6 +71,8 @@ __global__ void k_pair_pack(const PairPassArgs a) {
 }
 
 __global__ void k_pair_separate(const PairPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = (a.rows + 1) / 2;
     const bool cj = a.conj != 0;
     for (long long p = blockIdx.y; p < pairs; p += gridDim.y) {
@@ -78,6 +90,8 @@ __global__ void k_pair_separate(const PairPassArgs a) {
 }
 
 __global__ void k_pair_combine(const PairPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = (a.rows + 1) / 2;
     const bool fwd = a.conj != 0;
     for (long long p = blockIdx.y; p < pairs; p += gridDim.y) {
@@ -91,6 +105,8 @@ __global__ void k_pair_combine(const PairPassArgs a) {
 }
 
 __global__ void k_pair_split(const PairPassArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     const long long pairs = (a.rows + 1) / 2;
     for (long long p = blockIdx.y; p < pairs; p += gridDim.y) {
         const float2* z = static_cast<const float2*>(a.src) + p * a.in_pitch;
@@ -115,33 +131,27 @@ dim3 grid_for(long long per_row, long long rows, int block) {
 }  // namespace
 
 cudaError_t real_post(const RealPassArgs& a, cudaStream_t stream) {
-    k_real_post<<<grid_for(a.m / 2 + 1, a.rows, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_real_post, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a);
 }
 
 cudaError_t real_pre(const RealPassArgs& a, cudaStream_t stream) {
-    k_real_pre<<<grid_for(a.m / 2 + 1, a.rows, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_real_pre, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a);
 }
 
 cudaError_t pair_pack(const PairPassArgs& a, cudaStream_t stream) {
-    k_pair_pack<<<grid_for(a.n, (a.rows + 1) / 2, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_pair_pack, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
 }
 
 cudaError_t pair_separate(const PairPassArgs& a, cudaStream_t stream) {
-    k_pair_separate<<<grid_for(a.n / 2 + 1, (a.rows + 1) / 2, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_pair_separate, grid_for(a.n / 2 + 1, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
 }
 
 cudaError_t pair_combine(const PairPassArgs& a, cudaStream_t stream) {
-    k_pair_combine<<<grid_for(a.n, (a.rows + 1) / 2, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_pair_combine, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
 }
 
 cudaError_t pair_split(const PairPassArgs& a, cudaStream_t stream) {
-    k_pair_split<<<grid_for(a.n, (a.rows + 1) / 2, 256), 256, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_pair_split, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
 }
 
 }  // namespace sipfft

@@ -1210,6 +1210,8 @@ __global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a)
     const int tid = threadIdx.x;
     float2* bufs[2] = {sk_smem, sk_smem + (STAGES == 2 ? K::BUF : 0)};
     int tile = blockIdx.x;
+    grid_dep_wait();
+    grid_dep_launch();
     if (tile >= a.ntiles) return;
     // staged twiddles after the buffers (the barrier before pass 0 of the
     // first tile orders the copy before any use)

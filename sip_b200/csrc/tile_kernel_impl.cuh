@@ -97,6 +97,8 @@ __device__ __forceinline__ void tile_body(const TileArgs& a, int tile, int tid, 
 
 template <int SIGN, int E, int OP, bool TW4>
 __global__ void __launch_bounds__(kMaxTileThreads, 1) tile_fft_kernel(const TileArgs a) {
+    grid_dep_wait();
+    grid_dep_launch();
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x)
         tile_body<SIGN, E, OP, TW4>(a, tile, threadIdx.x, blockDim.x);
 }

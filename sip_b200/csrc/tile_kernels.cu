@@ -1,6 +1,9 @@
 // Host-side dispatch of the tile kernels compiled in tile_inst.cu.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
+#include "launch_attr.h"
 #include "tile_launch.h"
 
 namespace sipfft {
@@ -38,18 +41,25 @@ cudaError_t tile_prepare(int sign, int e, int op, bool tw4, int smem_bytes) {
                                 kMaxTileSmem);
 }
 
+// Read at every launch, so that a process can compare both forms.
+bool pdl_enabled() {
+    const char* e = std::getenv("SIP_FFT_PDL");
+    return e == nullptr || std::atoi(e) != 0;
+}
+
+// Both kernel families wait for the previous kernel of the stream before
+// touching global memory (grid_dep_wait), so both launch with PDL.
 cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream) {
     TileArgs a = L.args;
     a.src = src;
     a.dst = dst;
-    if (L.sk_fn != nullptr) {
-        void* params[] = {&a};
-        return cudaLaunchKernel(L.sk_fn, dim3(L.grid), dim3(L.block), params, (size_t)L.smem_bytes, stream);
-    }
-    KernelFn fn = pick_kernel(L.sign, L.e, L.op, L.tw4);
+    const void* fn = L.sk_fn;
+    if (fn == nullptr) fn = reinterpret_cast<const void*>(pick_kernel(L.sign, L.e, L.op, L.tw4));
     if (fn == nullptr) return cudaErrorInvalidValue;
-    fn<<<L.grid, L.block, L.smem_bytes, stream>>>(a);
-    return cudaGetLastError();
+    void* params[] = {&a};
+    cudaLaunchAttribute attr;
+    const cudaLaunchConfig_t cfg = pdl_config(dim3(L.grid), dim3(L.block), (size_t)L.smem_bytes, stream, &attr);
+    return cudaLaunchKernelExC(&cfg, fn, params);
 }
 
 cudaError_t sk_prepare(const void* fn, int smem_bytes, int block, int* ctas_per_sm) {

@@ -226,7 +226,7 @@ def test_partial_overlap_rejected(sip_lib, handle):
 
 
 @pytest.mark.parametrize("t,sizes,kinds", [
-    (C2C, [4096], ["c2c cluster"]),   # two transforms: one thread-block cluster each
+    (C2C, [4096], ["c2c rows"]),
     (C2C, [6000], ["c2c rows"]),
     (C2C, [65536], ["four-step A", "four-step B"]),
     (C2C, [2048, 2048], ["c2c axis 1", "c2c axis 0"]),

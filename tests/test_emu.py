@@ -127,9 +127,9 @@ def _plan_for_sk(op, mode, sign, tw4, n):
 def test_every_specialized_kernel(emu, monkeypatch):
     """Each compiled size-specialized kernel is selected by the planner and
     matches the FP64 oracle (including partial tiles and odd row counts).
-    The cluster form, which small C2C batches of some lengths take instead,
-    is switched off here (tests/test_emu_cluster.py covers it)."""
-    monkeypatch.setenv("SIP_FFT_CLUSTER", "0")
+    The opt-in cluster form stays off here (tests/test_emu_cluster.py
+    covers it)."""
+    monkeypatch.delenv("SIP_FFT_CLUSTER", raising=False)
     entries = _sk_list(emu)
     assert len(entries) >= 20
     emu.emu_set_real_fused.argtypes = [ctypes.c_int]

@@ -217,21 +217,26 @@ def test_odd_real_above_one_tile(cuda, n, op, direction, batch):
 @pytest.mark.parametrize("n,batch", [(1024, 1024), (4096, 256), (8192, 3), (4096, 1)])
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 def test_cluster_four_step(cuda, n, batch, direction, monkeypatch):
-    """Small C2C batches run one transform per thread-block cluster (the
-    CTAs exchanging through distributed shared memory); the same plan with
-    the cluster form switched off runs the one-CTA-per-transform kernel.
-    Both match FP64."""
+    """With SIP_FFT_CLUSTER=1, small C2C batches run one transform per
+    thread-block cluster (the CTAs exchanging through distributed shared
+    memory); by default the same plan runs the one-CTA-per-transform
+    kernel.  Both match FP64."""
     from tests.fftcase import random_input
     from sip_b200.fft import FftHandle
 
     x = random_input(O.C2C, [n], batch, seed=n + batch)
+    want = O.fp64(O.C2C, direction, x, [n])
+    monkeypatch.setenv("SIP_FFT_CLUSTER", "1")
     h = FftHandle()
     assert h.make_plan_1d(n, O.C2C, direction, batch) == 0
     assert h.describe()["steps"][0]["kind"] == 9   # the cluster step
     h.destroy()
-    want = O.fp64(O.C2C, direction, x, [n])
     out = gpu_run(cuda, O.C2C, direction, [n], batch, x)
     assert O.rel_l2(out, want) <= REL_L2_TOL
-    monkeypatch.setenv("SIP_FFT_CLUSTER", "0")
+    monkeypatch.delenv("SIP_FFT_CLUSTER")
+    h = FftHandle()
+    assert h.make_plan_1d(n, O.C2C, direction, batch) == 0
+    assert h.describe()["steps"][0]["kind"] != 9
+    h.destroy()
     out0 = gpu_run(cuda, O.C2C, direction, [n], batch, x)
     assert O.rel_l2(out0, want) <= REL_L2_TOL
