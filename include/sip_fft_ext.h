@@ -49,8 +49,11 @@ AsdSip::AspbStatus sipFftTakeDeviceErrors(unsigned* errors);
 #define SIP_FFT_HINT_RADIX_ORDER 4      /* 0: descending radices, 1: ascending */
 #define SIP_FFT_HINT_REAL_FUSED 5       /* real lengths above one tile: 0 default (R2C fused,
                                            C2R pre-process pass), 1 fuse both, 2 fuse neither */
-#define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant
-                                           (0 default; a step without that variant uses its default) */
+#define SIP_FFT_HINT_SK_VARIANT 6       /* which compiled size-specialized kernel variant: -1
+                                           (default) automatic (the first, or for a row step of
+                                           less than one wave of tiles the variant with more
+                                           threads per tile where one is compiled); 0..15 that
+                                           variant (a step without it uses its first) */
 #define SIP_FFT_HINT_RUNTIME_COMPILE 7  /* steps of a length without a compiled size-specialized
                                            kernel: 0 default (steps of >= 2^18 values use one compiled
                                            with NVRTC; a configuration not yet compiled is compiled in

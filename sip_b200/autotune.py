@@ -31,7 +31,7 @@ class Candidate:
     generic: int = 0  # 1: generic tile kernels only
     order: int = 0    # radix order (0 descending, 1 ascending)
     fused: int = 0    # real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
-    variant: int = 0  # compiled size-specialized variant
+    variant: int = -1  # compiled size-specialized variant (-1: automatic)
     jit: int = 0      # run-time compiled kernels: 0 default, 1 always, 2 never
 
     def line(self, fft_type: int, direction: int, sizes, batch: int) -> str:
@@ -41,7 +41,7 @@ class Candidate:
 
 
 def candidates(max_p: int = 16) -> list[Candidate]:
-    out = [Candidate(), Candidate(fused=1), Candidate(fused=2)] + [Candidate(variant=v) for v in (1, 2, 3)]
+    out = [Candidate(), Candidate(fused=1), Candidate(fused=2)] + [Candidate(variant=v) for v in (0, 1, 2, 3)]
     out += [Candidate(jit=1), Candidate(jit=2)]
     ps = [0] + [p for p in (1, 2, 4, 8, 16, 32) if p <= max_p]
     for p, e, order in itertools.product(ps, (16, 32), (0, 1)):

@@ -625,7 +625,7 @@ AspbStatus sipFftSetPlanHint(asdFftHandle handle, int key, int value) {
             p->hint_real_fused = value;
             break;
         case SIP_FFT_HINT_SK_VARIANT:
-            if (value < 0 || value > 15) return ACL_ERROR_INVALID_PARAM;
+            if (value < -1 || value > 15) return ACL_ERROR_INVALID_PARAM;
             p->hint_sk_variant = value;
             break;
         case SIP_FFT_HINT_RUNTIME_COMPILE:

@@ -264,7 +264,11 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     // ("25,15,8", must multiply to n), SIP_FFT_JIT_P, SIP_FFT_JIT_T,
     // SIP_FFT_JIT_MINB, SIP_FFT_JIT_STAGES, SIP_FFT_JIT_TWB (the SK_TW_* bits
     // of sk_kernel.cuh: basis table, twiddles in shared memory, mirrored pairs).
-    if (const char* rs = std::getenv("SIP_FFT_JIT_RADICES")) {
+    // With SIP_FFT_JIT_PREFER=<length> they apply to steps of that length only.
+    const int only_n = env_int("SIP_FFT_JIT_PREFER", 0);
+    const bool ovr = only_n <= 1 || only_n == n;
+    auto ovr_int = [&](const char* name, int dflt) { return ovr ? env_int(name, dflt) : dflt; };
+    if (const char* rs = ovr ? std::getenv("SIP_FFT_JIT_RADICES") : nullptr) {
         std::vector<int> r;
         long long prod = 1;
         for (const char* q = rs; *q;) {
@@ -295,8 +299,8 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
         P = std::max<long long>(1, P / 2);
     }
     if (T > kMaxTileThreads) return false;
-    if (env_int("SIP_FFT_JIT_P", 0) > 0) P = std::min<long long>(env_int("SIP_FFT_JIT_P", 0), transforms);
-    if (env_int("SIP_FFT_JIT_T", 0) > 0) T = env_int("SIP_FFT_JIT_T", 0);
+    if (ovr_int("SIP_FFT_JIT_P", 0) > 0) P = std::min<long long>(ovr_int("SIP_FFT_JIT_P", 0), transforms);
+    if (ovr_int("SIP_FFT_JIT_T", 0) > 0) T = ovr_int("SIP_FFT_JIT_T", 0);
     if (T % 32 != 0 || T > kMaxTileThreads) return false;
     c.P = (int)P;
     c.T = T;
@@ -304,7 +308,7 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     c.LD = sk_pitch(n, r0);
     // twiddle options (SK_TW_* bits; SIP_FFT_JIT_TWB overrides them): mirrored
     // butterfly pairs apply to real half-length tiles of two or more passes
-    c.twb = env_int("SIP_FFT_JIT_TWB", c.twb);
+    c.twb = ovr_int("SIP_FFT_JIT_TWB", c.twb);
     if (c.twb < 0 || c.twb > 15) return false;
     if ((c.twb & SK_MIRROR_PAIR) && (!real_op || c.radices.size() < 2)) c.twb &= ~SK_MIRROR_PAIR;
     if ((c.twb & SK_SPLIT_PASS0) && (c.radices.size() < 2 || op == OP_PC)) c.twb &= ~SK_SPLIT_PASS0;
@@ -314,12 +318,12 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     if (2 * buf + tws <= kMaxTileSmem) c.stages = 2;
     else if (buf + tws <= kMaxTileSmem) c.stages = 1;
     else return false;
-    if (env_int("SIP_FFT_JIT_STAGES", 0) == 1) c.stages = 1;
+    if (ovr_int("SIP_FFT_JIT_STAGES", 0) == 1) c.stages = 1;
     if (c.stages != 2) c.twb &= ~SK_SPLIT_PASS0;  // a split pass 0 uses the second buffer as its work layout
     c.smem = (int)(c.stages * buf + tws);
     const int smem_ctas = std::max<int>(1, (228 * 1024) / (c.smem + 1024));
     c.minb = std::max(1, std::min(65536 / (T * 128), smem_ctas));
-    if (env_int("SIP_FFT_JIT_MINB", 0) > 0) c.minb = env_int("SIP_FFT_JIT_MINB", 0);
+    if (ovr_int("SIP_FFT_JIT_MINB", 0) > 0) c.minb = ovr_int("SIP_FFT_JIT_MINB", 0);
     *out = c;
     return true;
 }

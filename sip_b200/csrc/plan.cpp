@@ -48,7 +48,7 @@ int64_t FftPlan::elements() const {
 namespace {
 thread_local int g_compute_mode = kComputeFp32;
 thread_local int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0,
-                 g_hint_variant = 0, g_hint_jit = 0;
+                 g_hint_variant = -1, g_hint_jit = 0;
 }  // namespace
 
 // ------------------------------------------------------------ radices
@@ -222,9 +222,11 @@ void try_specialize(Step& st, const AxisIO& io) {
     const int mode = sk_mode_of(L.op, a.N, io, (a.flags & TF_BLUE) ? a.n_other : 0);
     if (mode < 0) return;
     // SIP_FFT_JIT_PREFER=1 (tuning sweeps) skips the compiled kernels so that
-    // run-time configurations can be timed against them
+    // run-time configurations can be timed against them; =<length> does so
+    // for steps of that length only
     const char* prefer = std::getenv("SIP_FFT_JIT_PREFER");
-    const bool prefer_jit = prefer != nullptr && std::strcmp(prefer, "1") == 0;
+    const int prefer_n = prefer != nullptr ? std::atoi(prefer) : 0;
+    const bool prefer_jit = prefer_n == 1 || (prefer_n > 1 && prefer_n == a.N);
     const SkEntry* e = prefer_jit ? nullptr : sk_find(L.op, mode, L.sign, L.tw4, a.N, g_hint_variant);
     // No compiled kernel for this length: a run-time compiled one (jit.cpp)
     // for steps large enough to repay the compilation, or on request.
@@ -237,6 +239,15 @@ void try_specialize(Step& st, const AxisIO& io) {
         e = sk_jit_entry(L.op, mode, L.sign, L.tw4, a.N, io.inner, sync);
     }
     if (e == nullptr) return;
+    // A row step of less than one wave of tiles (two per SM) takes the
+    // compiled variant with more threads per tile when there is one: each
+    // transform's loads, passes and stores spread over more warps (C2C 4096
+    // x 256: 7.2 us with 256 threads per transform, 8.7 us with 128).
+    if (g_hint_variant < 0 && mode == SK_ROWS && !e->jit) {
+        const long long tiles = (io.inner + e->P - 1) / e->P * io.outer;
+        if (tiles <= kOneWaveTiles)
+            if (const SkEntry* w = sk_find_wider(e)) e = w;
+    }
     st.sk = e;
     st.radices = e->radices;
     int tw_entries = 0;
@@ -339,6 +350,14 @@ bool four_step_split(long long n, int* n1, int* n2) {
         best1 = (int)a;  // ascending a: the last hit is the most balanced
     }
     if (best1 == 0) return false;
+    // SIP_FFT_SPLIT_N1 (tuning sweeps): the column length, when it divides n
+    // into two lengths that fit a tile
+    if (const char* e = std::getenv("SIP_FFT_SPLIT_N1")) {
+        const long long a = std::atoll(e);
+        if (a >= 2 && n % a == 0 && a <= kMaxTileN && n / a <= kMaxTileN && factorizable((int)a, 32) &&
+            factorizable((int)(n / a), 32))
+            best1 = (int)a;
+    }
     *n1 = best1;
     *n2 = (int)(n / best1);
     return true;
@@ -1098,7 +1117,7 @@ bool apply_tune_cache(FftPlan& plan) {
             plan.hint_generic = gen;
             plan.hint_order = order;
             plan.hint_real_fused = got >= 9 ? fused : 0;
-            plan.hint_sk_variant = got >= 10 ? variant : 0;
+            plan.hint_sk_variant = got >= 10 ? variant : -1;
             plan.hint_jit = got >= 11 ? jit : 0;
             hit = true;  // the last matching line wins
         }

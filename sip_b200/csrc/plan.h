@@ -145,7 +145,7 @@ struct FftPlan {
     int hint_generic = 0;  // 1: generic tile kernels only (no size-specialized / tensor-core)
     int hint_order = 0;    // radix order: 0 descending, 1 ascending
     int hint_real_fused = 0;  // real lengths above one tile: 0 default, 1 fuse both, 2 fuse neither
-    int hint_sk_variant = 0;  // which compiled size-specialized variant (sk_configs.h order)
+    int hint_sk_variant = -1;  // compiled size-specialized variant (sk_configs.h order); -1 automatic
     int hint_jit = 0;  // run-time compiled sk kernels: 0 default (large steps), 1 always, 2 never
     bool hints_explicit = false;
     // Pulse-compression plan (sipFftMakePlanPulse1D): x -> IFFT(FFT(x) * F)
@@ -184,6 +184,8 @@ std::vector<int> choose_radices(int n, int e);
 
 // Largest complex length one tile kernel transforms (shared memory bound).
 constexpr int kMaxTileN = 16384;
+// Tiles of one wave on B200 at two CTAs per SM (148 SMs).
+constexpr long long kOneWaveTiles = 2 * 148;
 
 constexpr int kComputeFp32 = 0;
 constexpr int kPulseConj = 1;   // multiply by conj(F)

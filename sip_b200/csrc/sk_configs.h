@@ -82,6 +82,14 @@
     /* hint variants of the multi-pass steps: split pass 0 (TWB 8) or more, \
        smaller CTAs per SM */                                                 \
     X(0, 1024, 8, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 3, 32, 32)             \
+    /* the split 2^19 = 1024 x 512: columns of 1024 (pass A), R2C pass B +  \
+       post on rows of 512, C2C pass B on rows of 512 */                     \
+    X(6, 1024, 8, 256, OP_C2C, SK_COLS, -1, true, 1, 3, 1, 32, 32)                   \
+    X(7, 1024, 8, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 1, 32, 32)                    \
+    X(2, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 1, 16, 32)             \
+    X(3, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 1, 1, 16, 32)             \
+    X(4, 512, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 16, 32)                 \
+    X(5, 512, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 16, 32)                \
     X(1, 1024, 4, 128, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 3, 11, 32, 32)            \
     X(2, 512, 8, 128, OP_C2C, SK_COLS, -1, true, 2, 3, 9, 16, 32)                   \
     X(3, 512, 8, 128, OP_C2C, SK_COLS, 1, true, 2, 3, 9, 16, 32)                    \
@@ -89,6 +97,10 @@
     X(5, 1024, 4, 128, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 9, 32, 32)                 \
     X(6, 256, 16, 256, OP_C2C, SK_COLS, -1, true, 2, 3, 9, 16, 16)                   \
     X(7, 256, 16, 256, OP_C2C, SK_COLS, 1, true, 2, 3, 9, 16, 16)                    \
+    /* C2C 4096 rows, 256 threads per transform: taken automatically by row  \
+       steps of less than one wave of tiles (plan.cpp try_specialize) */     \
+    X(6, 4096, 1, 256, OP_C2C, SK_ROWS, -1, false, 2, 2, 9, 16, 16, 16)              \
+    X(7, 4096, 1, 256, OP_C2C, SK_ROWS, 1, false, 2, 2, 9, 16, 16, 16)               \
     X(0, 256, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 9, 16, 16)                \
     X(1, 256, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 9, 16, 16)                 \
     X(2, 256, 16, 256, OP_C2C, SK_COLS, -1, false, 2, 3, 9, 16, 16)                  \

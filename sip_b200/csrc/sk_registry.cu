@@ -33,6 +33,7 @@ const std::vector<SkEntry>& sk_registry() {
 }
 
 const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant) {
+    if (variant < 0) variant = 0;
     const SkEntry* first = nullptr;
     for (const SkEntry& e : sk_registry()) {
         if (e.op != op || e.mode != mode || e.sign != sign || e.tw4 != tw4 || e.n != n) continue;
@@ -40,6 +41,14 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant)
         if (variant-- == 0) return &e;
     }
     return first;
+}
+
+const SkEntry* sk_find_wider(const SkEntry* e) {
+    for (const SkEntry& x : sk_registry())
+        if (x.op == e->op && x.mode == e->mode && x.sign == e->sign && x.tw4 == e->tw4 && x.n == e->n &&
+            x.P == e->P && x.T > e->T)
+            return &x;
+    return nullptr;
 }
 
 }  // namespace sipfft

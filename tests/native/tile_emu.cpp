@@ -294,6 +294,7 @@ const std::vector<SkEntry>& sk_registry() {
 }
 const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant) {
     if (std::getenv("SIP_EMU_GENERIC_ONLY")) return nullptr;
+    if (variant < 0) variant = 0;
     const SkEntry* first = nullptr;
     for (const SkEntry& e : sk_registry()) {
         if (e.op != op || e.mode != mode || e.sign != sign || e.tw4 != tw4 || e.n != n) continue;
@@ -301,6 +302,13 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant)
         if (variant-- == 0) return &e;
     }
     return first;
+}
+const SkEntry* sk_find_wider(const SkEntry* e) {
+    for (const SkEntry& x : sk_registry())
+        if (x.op == e->op && x.mode == e->mode && x.sign == e->sign && x.tw4 == e->tw4 && x.n == e->n &&
+            x.P == e->P && x.T > e->T)
+            return &x;
+    return nullptr;
 }
 const ClEntry* cluster_find(int n, int sign) {
     static const std::vector<ClEntry> reg = [] {
@@ -543,7 +551,7 @@ int emu_run_plan(FftPlan& p, const void* in, void* out, char* desc, size_t desc_
 static int g_emu_real_fused = 0;
 void emu_set_real_fused(int v) { g_emu_real_fused = v; }
 // Planner sk-variant hint applied likewise.
-static int g_emu_sk_variant = 0;
+static int g_emu_sk_variant = -1;
 void emu_set_sk_variant(int v) { g_emu_sk_variant = v; }
 // Output shift (mode, scale) applied likewise.
 static int g_emu_shift = 0;

@@ -28,7 +28,7 @@ def test_fastest_candidate_is_cached_and_read_back(tmp_path):
     r = tune(L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, [4096], 64, str(cache),
              timer=lambda c: 1.0 if c == want else 2.0)
     assert r["best"] == want
-    assert cache.read_text() == "16 16 4096 64 2 32 1 1 0 0 0\n"
+    assert cache.read_text() == "16 16 4096 64 2 32 1 1 0 -1 0\n"
     code = ("import sys,json; sys.path.insert(0, %r); from sip_b200.fft import FftHandle; h=FftHandle(); "
             "h.make_plan_1d(4096, 0x10, 0x10, 64); s=h.describe()['steps'][0]; "
             "print(json.dumps([s['sk'], s['e'], s['P'], s['radices']]))" % str(ROOT))

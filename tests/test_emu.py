@@ -124,6 +124,16 @@ def _plan_for_sk(op, mode, sign, tw4, n):
     return O.C2C, d, [split[n]], 1
 
 
+def _split_n1(op, mode, tw4, n):
+    """Column length of the four-step split that uses this kernel, when it
+    is not the planner's default (2^19 = 512 x 1024)."""
+    if n == 512 and ((op == 5 and mode == 2) or (op == 0 and mode == 2)):
+        return 1024   # rows of 512
+    if n == 1024 and op == 0 and mode == 1 and tw4:
+        return 1024   # columns of 1024
+    return None
+
+
 def test_every_specialized_kernel(emu, monkeypatch):
     """Each compiled size-specialized kernel is selected by the planner and
     matches the FP64 oracle (including partial tiles and odd row counts).
@@ -145,11 +155,16 @@ def test_every_specialized_kernel(emu, monkeypatch):
         seen[key] = variant + 1
         emu.emu_set_real_fused(1 if op == 6 else 0)  # the fused C2R form is selected by hint
         emu.emu_set_sk_variant(variant)
+        n1 = _split_n1(op, mode, tw4, n)
+        if n1:
+            monkeypatch.setenv("SIP_FFT_SPLIT_N1", str(n1))
+        else:
+            monkeypatch.delenv("SIP_FFT_SPLIT_N1", raising=False)
         try:
             rc, out, desc = emu_run(emu, typ, d, sizes, batch, x)
         finally:
             emu.emu_set_real_fused(0)
-            emu.emu_set_sk_variant(0)
+            emu.emu_set_sk_variant(-1)
         assert rc == 0, desc
         import json
 
