@@ -19,6 +19,17 @@ extern "C" {
  * every check of asdFftExecC2C/R2C/C2R except the tensor shape match. */
 AsdSip::AspbStatus sipFftExecRaw(AsdSip::asdFftHandle handle, const void* input, void* output);
 
+/* Executes a planned 1-D or pulse-compression handle on its first `rows`
+ * transforms only (1 <= rows <= the plan's batch), with the intermediate in
+ * `workspace` when it is not NULL (at least the plan's workspace size; NULL:
+ * the bound workspace, under the usual workspace protocol).  Lets a caller
+ * keep one resident plan per length and run requests of any smaller batch
+ * through it (the serving loop does).  API_NOT_SUPPORT for multi-D plans and
+ * plans with steps that cannot be limited to rows (Bluestein lengths, odd
+ * real lengths above one tile, the cluster and tensor-core forms). */
+AsdSip::AspbStatus sipFftExecRawRows(AsdSip::asdFftHandle handle, long long rows, const void* input, void* output,
+                                     void* workspace);
+
 /* Writes a JSON description of the plan's kernel steps into buf (always
  * NUL-terminated when cap > 0) and the full length + 1 into *needed. */
 AsdSip::AspbStatus sipFftDescribePlan(AsdSip::asdFftHandle handle, char* buf, size_t cap, size_t* needed);

@@ -73,7 +73,7 @@ EXPORTED = [
     "sipFftSetPlanHint", "sipFftBatchCreate", "sipFftBatchDestroy", "sipFftBatchClear", "sipFftBatchAdd",
     "sipFftBatchExec", "sipFftBatchSetGate", "sipFftBatchUseGraphs", "sipFftBatchTakeStatus",
     "sipFftExecC2CNoAlloc", "sipFftMakePlanPulse1D", "sipFftBatchAddRows", "sipFftSetOutputShift",
-    "sipFftJitCompileCheck", "sipFftJitWait",
+    "sipFftJitCompileCheck", "sipFftJitWait", "sipFftExecRawRows",
     "aclCreateTensor", "aclDestroyTensor", "aclGetViewShape", "aclGetDataType", "aclFreeViewShape",
     "aclGetTensorData",
 ]
@@ -104,6 +104,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "asdFftShift": (_i32, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
         "asdIfftShift": (_i32, [_i64, _i64, _i64, _i64, ctypes.c_double, _vp, _vp, _vp, _vp]),
         "sipFftExecRaw": (_i32, [_vp, _vp, _vp]),
+        "sipFftExecRawRows": (_i32, [_vp, ctypes.c_longlong, _vp, _vp, _vp]),
         "sipFftDescribePlan": (_i32, [_vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
         "sipFftVersion": (ctypes.c_char_p, []),
         "sipFftSetComputeMode": (_i32, [_vp, ctypes.c_int]),

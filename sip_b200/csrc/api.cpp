@@ -551,6 +551,47 @@ AspbStatus sipFftExecRaw(asdFftHandle handle, const void* input, void* output) {
     return exec_plan(*p, input, output);
 }
 
+AspbStatus sipFftExecRawRows(asdFftHandle handle, long long rows, const void* input, void* output,
+                             void* workspace) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    FftPlan* p = find_plan(handle);
+    if (p == nullptr || !p->initialized || rows < 1 || rows > p->batch) return ACL_ERROR_INVALID_PARAM;
+    if (!sipfft::rows_exec_supported(*p)) return ACL_ERROR_API_NOT_SUPPORT;
+    void* ws = workspace != nullptr ? workspace : p->workspace;
+    if (p->workspace_need > 0) {
+        if (ws == nullptr) {
+            std::fprintf(stderr, "[sip_b200] workspace has not been set\n");
+            return ACL_ERROR_INTERNAL_ERROR;
+        }
+        if (workspace == nullptr && p->workspace_recorded == 0) {
+            std::fprintf(stderr, "[sip_b200] call asdFftGetWorkspaceSize before exec\n");
+            return ACL_ERROR_INVALID_PARAM;
+        }
+    }
+    if (input == nullptr || output == nullptr) return ACL_ERROR_INTERNAL_ERROR;
+    const char* ib = static_cast<const char*>(input);
+    const char* ob = static_cast<const char*>(output);
+    const size_t isz = operand_bytes(*p, true) / (size_t)p->batch * (size_t)rows;
+    const size_t osz = operand_bytes(*p, false) / (size_t)p->batch * (size_t)rows;
+    const bool overlap = ib < ob + osz && ob < ib + isz;
+    if (overlap && !(ib == ob && p->type == ASCEND_FFT_C2C)) {
+        std::fprintf(stderr, "[sip_b200] input and output overlap\n");
+        return ACL_ERROR_INVALID_PARAM;
+    }
+    try {
+        if (!p->resources_ready) {
+            if (!device_present()) return ACL_ERROR_INTERNAL_ERROR;
+            sipfft::prepare_device(*p);
+        }
+        DeviceGuard g(p->device);
+        sipfft::launch_rows(*p, rows, input, output, ws);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[sip_b200] exec failed: %s\n", e.what());
+        return ACL_ERROR_INTERNAL_ERROR;
+    }
+    return ACL_SUCCESS;
+}
+
 AspbStatus sipFftDescribePlan(asdFftHandle handle, char* buf, size_t cap, size_t* needed) {
     std::lock_guard<std::mutex> lk(g_mu);
     FftPlan* p = find_plan(handle);

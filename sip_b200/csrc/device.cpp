@@ -353,6 +353,13 @@ void launch_one(const Step& st, cudaStream_t stream, const void* in, void* out, 
 
 }  // namespace
 
+// A row-limited exec: every step as chunk units [0, rows) (a unit is one
+// batch row in 1-D and pulse plans), workspace regions at their start.
+void launch_rows(const FftPlan& plan, long long rows, const void* in, void* out, void* ws) {
+    cudaStream_t stream = static_cast<cudaStream_t>(plan.stream);
+    for (const Step& st : plan.steps) launch_one(st, stream, in, out, ws, 0, rows);
+}
+
 // Steps of a chunk group run chunk by chunk: every step of the group on
 // units [u0, u0 + cu), then the next chunk.  The workspace regions of the
 // group are reused by every chunk, so the intermediate one step writes and

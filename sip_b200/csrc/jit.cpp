@@ -511,8 +511,10 @@ std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, 
 
 bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out,
                    std::string* err) {
-    // The candidates are compiled concurrently; the first in order without
-    // register spills wins, else the one with the fewest spilled bytes.
+    // The first candidate in order without register spills wins, else the
+    // one with the fewest spilled bytes.  The first is compiled alone (it
+    // wins whenever it does not spill, which saves the others' compilation
+    // time); only when it spills are the others compiled, concurrently.
     const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms);
     if (cands.empty()) {
         *err = "no run-time configuration for this step";
@@ -524,13 +526,18 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
         std::string err;
     };
     std::vector<Result> res(cands.size());
+    auto compile = [&](size_t i) {
+        std::vector<char> cubin;
+        std::string lowered;
+        res[i].ok = sk_jit_compile(cands[i], &cubin, &lowered, &res[i].err, &res[i].spill);
+    };
+    compile(0);
+    if (res[0].ok && res[0].spill == 0) {
+        *out = cands[0];
+        return true;
+    }
     std::vector<std::thread> workers;
-    for (size_t i = 0; i < cands.size(); ++i)
-        workers.emplace_back([&, i] {
-            std::vector<char> cubin;
-            std::string lowered;
-            res[i].ok = sk_jit_compile(cands[i], &cubin, &lowered, &res[i].err, &res[i].spill);
-        });
+    for (size_t i = 1; i < cands.size(); ++i) workers.emplace_back(compile, i);
     for (auto& w : workers) w.join();
     int best = -1;
     for (size_t i = 0; i < cands.size(); ++i) {
@@ -602,8 +609,8 @@ bool select_cached(const std::vector<JitCfg>& cands, JitCfg* out) {
     return true;
 }
 
-// Background compilation: a FIFO of steps served by two detached worker
-// threads.  The state is never destroyed, so a worker still compiling while
+// Background compilation: a FIFO of steps served by detached worker threads
+// (2, or SIP_FFT_JIT_THREADS, at most 64).  The state is never destroyed, so a worker still compiling while
 // the process exits touches no destroyed object; an exit handler (registered
 // after NVRTC is loaded, so it runs before NVRTC's own teardown) stops the
 // queue and waits up to 30 s for the jobs already running.  A fork waits
@@ -624,7 +631,8 @@ struct JitWorkers {
     void start() {  // with mu held
         if (started) return;
         started = true;
-        for (int i = 0; i < 2; ++i)
+        const int nthreads = std::max(1, std::min(64, env_int("SIP_FFT_JIT_THREADS", 2)));
+        for (int i = 0; i < nthreads; ++i)
             std::thread([this] {
                 for (;;) {
                     std::function<void()> job;

@@ -1201,13 +1201,16 @@ void form_chunk_groups(FftPlan& plan) {
     plan.chunk_groups.clear();
     for (Step& st : plan.steps) st.chunk_group = -1;
     const size_t ns = plan.steps.size();
-    if (ns < 2) return;
-    if (plan.sizes.size() == 1 || plan.pulse) {
+    // 1-D and pulse plans: a chunk unit is one batch row in every step (also
+    // what a row-limited exec, launch_rows, runs on)
+    if (plan.sizes.size() == 1 || plan.pulse)
         for (Step& st : plan.steps)
             if (st.kind == StepKind::Tile) {
                 st.chunk_dim = st.batch_dim;
                 st.chunk_per = 1;
             }
+    if (ns < 2) return;
+    if (plan.sizes.size() == 1 || plan.pulse) {
         make_chunk_group(plan, 0, ns, plan.batch);
         return;
     }
@@ -1295,6 +1298,19 @@ long long exec_launches(const FftPlan& plan) {
         }
     }
     return n;
+}
+
+bool rows_exec_supported(const FftPlan& plan) {
+    if (plan.sizes.size() != 1 && !plan.pulse) return false;
+    for (const Step& st : plan.steps) {
+        if (st.kind == StepKind::Tile) {
+            if (st.chunk_dim != 1 && st.chunk_dim != 2) return false;
+            if (st.L.op == OP_R2C_PAIR || st.L.op == OP_C2R_PAIR) return false;
+        } else if (st.kind != StepKind::RealPre && st.kind != StepKind::RealPost) {
+            return false;
+        }
+    }
+    return true;
 }
 
 TileLaunch chunk_tile_launch(const Step& st, long long cnt) {

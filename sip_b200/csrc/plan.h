@@ -228,6 +228,13 @@ void launch_separated(const FftPlan& plan, const float* in_re, const float* in_i
 // Launches every step on the plan's stream (chunk groups chunk by chunk).
 void launch_steps(const FftPlan& plan, const void* in, void* out, void* ws);
 
+// True when every step of the plan can run on the first rows of its batch
+// alone (1-D and pulse plans of tile and real pre/post steps).
+bool rows_exec_supported(const FftPlan& plan);
+// Every step of the plan over the first `rows` transforms of its batch,
+// 1 <= rows <= plan.batch, with workspace `ws`.
+void launch_rows(const FftPlan& plan, long long rows, const void* in, void* out, void* ws);
+
 // Chunk units per chunk of a group for the current L2 chunk size
 // (SIP_FFT_L2_CHUNK_MB, default kL2ChunkBytes; 0 turns chunking off); the
 // group's `units` when it runs as one launch per step.

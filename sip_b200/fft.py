@@ -138,6 +138,11 @@ class FftHandle:
     def exec_raw(self, in_ptr: int, out_ptr: int) -> int:
         return self.lib.sipFftExecRaw(self.h, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr))
 
+    def exec_rows(self, rows: int, in_ptr: int, out_ptr: int, ws_ptr: int | None = None) -> int:
+        """The plan on its first `rows` transforms (sipFftExecRawRows)."""
+        return self.lib.sipFftExecRawRows(self.h, ctypes.c_longlong(rows), ctypes.c_void_p(in_ptr),
+                                          ctypes.c_void_p(out_ptr), ctypes.c_void_p(ws_ptr or 0))
+
     def synchronize(self) -> int:
         return self.lib.asdFftSynchronize(self.h)
 

@@ -15,6 +15,12 @@ Two executors share the scheduler:
     launch per pass index for the whole group, replayed from a captured CUDA
     graph, with the fused pulse-compression kernels; one plan per length
     (batch 512) serves any batch through sipFftBatchAddRows.
+  * `ResidentExecutor`: the same resident plans (one per length, batch
+    512) on the size-specialized and run-time compiled kernels instead of
+    the queue's generic tile body; every request of a group runs its rows
+    through its length's plan (sipFftExecRawRows), the group's launches on
+    one of several streams (launches of consecutive requests overlap through
+    programmatic dependent launch).
   * `PlainExecutor`: the plain per-request FP32 path, as a user of the
     reference's API writes it: per request a forward C2C exec, an
     elementwise multiply, an inverse C2C exec, with plans kept in an LRU
@@ -411,6 +417,85 @@ class QueueExecutor(_GpuBase):
             b.destroy()
         for h in self.plans.values():
             h.destroy()
+
+
+class ResidentExecutor(_GpuBase):
+    """Groups through resident per-length plans on the specialized kernels,
+    one row-limited exec per request."""
+
+    def __init__(self, torch, budget_bytes: int, lengths, max_batch: int = 512, streams: int = 4,
+                 jit_wait_ms: int = 600_000, device=None):
+        super().__init__(torch, budget_bytes, device)
+        from . import _lib as L
+        from .fft import check
+
+        self.L = L
+        self.check = check
+        self.max_batch = max_batch
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
+        self.slot_event = [None] * streams
+        self.next = 0
+        self.plans = {}
+        # The first plans start the run-time compilation of every length's
+        # kernels in the background; the plans made after it has finished
+        # use them (a plan keeps the kernels it was made with).
+        self._make_plans(lengths)
+        check(L.lib().sipFftJitWait(jit_wait_ms), "run-time kernels")
+        self._destroy_plans()
+        self._make_plans(lengths)
+        self.launches = 0
+
+    def _make_plans(self, lengths):
+        from .fft import FftHandle
+
+        L, check = self.L, self.check
+        for n in lengths:
+            for kind in (KIND_PULSE, KIND_FFT):
+                h = FftHandle()
+                if kind == KIND_PULSE:
+                    check(h.make_plan_pulse_1d(n, self.max_batch, self.filter(n).data_ptr(),
+                                               L.SIP_FFT_PULSE_CONJ_FILTER), "pulse plan")
+                else:
+                    check(h.make_plan_1d(n, L.ASCEND_FFT_C2C, L.ASCEND_FFT_FORWARD, self.max_batch), "fft plan")
+                check(h.workspace_size()[0], "workspace size")
+                self.plans[(kind, n)] = h
+
+    def _destroy_plans(self):
+        for h in self.plans.values():
+            h.destroy()
+        self.plans.clear()
+
+    def _free_slot(self) -> int:
+        for k in range(len(self.streams)):
+            i = (self.next + k) % len(self.streams)
+            ev = self.slot_event[i]
+            if ev is None or ev.query():
+                return i
+        return self.next
+
+    def launch(self, group):
+        torch = self.torch
+        i = self._free_slot()
+        self.next = (i + 1) % len(self.streams)
+        s = self.streams[i]
+        check = self.check
+        with torch.cuda.stream(s):
+            for r in group:
+                self.make_signal(r, self.view(self.regions(r)[0], r.batch * r.n))
+        for r in group:
+            x, y, ws = self.regions(r)
+            h = self.plans[(r.kind, r.n)]
+            check(h.set_stream(s), "stream")
+            check(h.exec_rows(r.batch, self.base + x, self.base + y, self.base + ws if ws is not None else None),
+                  "exec rows")
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(s)
+        self.slot_event[i] = ev
+        self.launches += 1
+        return ev
+
+    def close(self) -> None:
+        self._destroy_plans()
 
 
 class PlainExecutor(_GpuBase):

@@ -346,3 +346,24 @@ def test_bluestein_limit(sip_lib, handle):
     assert desc_ok == OK
     steps = describe(sip_lib, handle)["steps"]
     assert steps[0]["m"] == 1 << 28
+
+
+def test_rows_exec_checks(sip_lib, handle):
+    """sipFftExecRawRows: rows outside [1, batch] and unplanned handles are
+    INVALID_PARAM; plans whose steps cannot be limited to rows (multi-D,
+    Bluestein lengths) are API_NOT_SUPPORT; all before touching a device."""
+    x, y = ctypes.c_void_p(0x10000), ctypes.c_void_p(0x40000000)
+    assert sip_lib.sipFftExecRawRows(handle, 1, x, y, None) == INV   # not planned
+    assert plan1d(sip_lib, handle, 4096, C2C, F, 8) == OK
+    for rows in (0, -1, 9):
+        assert sip_lib.sipFftExecRawRows(handle, rows, x, y, None) == INV
+    h2 = ctypes.c_void_p()
+    assert sip_lib.asdFftCreate(ctypes.byref(h2)) == OK
+    assert sip_lib.asdFftMakePlan2D(h2, 64, 64, C2C, F, 2) == OK
+    assert sip_lib.sipFftExecRawRows(h2, 1, x, y, None) == NOTSUP
+    sip_lib.asdFftDestroy(h2)
+    h3 = ctypes.c_void_p()
+    assert sip_lib.asdFftCreate(ctypes.byref(h3)) == OK
+    assert plan1d(sip_lib, h3, 100003, C2C, F, 2) == OK   # prime: Bluestein steps
+    assert sip_lib.sipFftExecRawRows(h3, 1, x, y, None) == NOTSUP
+    sip_lib.asdFftDestroy(h3)

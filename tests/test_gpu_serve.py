@@ -65,3 +65,33 @@ def test_serving_latency_stats(cuda):
     assert s["requests"] == 200 and 0 < s["p50_ms"] <= s["p99_ms"]
     assert all(r.done >= r.arrival for r in reqs)
     ex.close()
+
+
+def test_resident_executor_mix_equals_alone(cuda):
+    """The resident executor (specialized kernels, one row-limited exec per
+    request): each request's result is the same in the mix as alone and
+    matches the FP64 oracle."""
+    from sip_b200.serve import ResidentExecutor
+
+    torch = cuda
+    reqs = make_requests(30, rate_hz=float("inf"), seed=13, lo=256, hi=1 << 17, max_batch=24, fft_share=0.3)
+    lengths = sorted({r.n for r in reqs})
+    budget = 160 << 20
+    ex = ResidentExecutor(torch, budget, lengths, max_batch=24, streams=2)
+    saved = {}
+
+    def keep(group):
+        for r in group:
+            saved[r.rid] = (ex.input(r).clone(), ex.output(r).clone())
+
+    stats = Scheduler(ex, budget, max_inflight=2, on_complete=keep).run(reqs)
+    assert len(stats.requests) == len(reqs) and stats.max_group > 1
+    for r in reqs:
+        x, y = saved[r.rid]
+        alone = Request(r.rid, r.kind, r.n, r.batch, 0.0, r.delay)
+        got = {}
+        ex.fixed[r.rid] = x
+        Scheduler(ex, budget, on_complete=lambda g: got.update({q.rid: ex.output(q).clone() for q in g})).run([alone])
+        assert torch.equal(got[r.rid], y), (r.kind, r.n, r.batch)
+        assert O.rel_l2(y.cpu().numpy(), want(r, x.cpu().numpy())) <= REL_L2_TOL, (r.kind, r.n, r.batch)
+    ex.close()
