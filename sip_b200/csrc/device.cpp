@@ -201,7 +201,14 @@ ChunkLanes::~ChunkLanes() {
 void prepare_device(FftPlan& plan) {
     int device = -1;
     check(cudaGetDevice(&device), "cudaGetDevice");
-    if (!plan.chunk_groups.empty()) {
+    // The second lane (a stream and two events) only for plans that run in
+    // chunks under the current settings: creating and destroying a stream
+    // costs a few hundred microseconds, which plans made per request (a
+    // serving loop's plain path) would pay every time.  A plan without it
+    // runs its chunks on one lane.
+    bool chunked = false;
+    for (const ChunkGroup& g : plan.chunk_groups) chunked = chunked || chunk_units(g) < g.units;
+    if (chunked) {
         auto l = std::make_shared<ChunkLanes>();
         check(cudaStreamCreateWithFlags(&l->side, cudaStreamNonBlocking), "cudaStreamCreate");
         check(cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming), "cudaEventCreate");

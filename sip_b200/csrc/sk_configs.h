@@ -88,6 +88,10 @@
     X(7, 1024, 8, 256, OP_C2C, SK_COLS, 1, true, 1, 3, 1, 32, 32)                    \
     X(2, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 1, 16, 32)             \
     X(3, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 1, 1, 16, 32)             \
+    /* R2C pass B with the post-process on mirrored butterfly pairs (TWB 5): \
+       rows of 512 (split 1024 x 512) and of 1024 (split 512 x 1024) */      \
+    X(4, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 5, 32, 16)             \
+    X(5, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 5, 16, 4, 16)         \
     X(4, 512, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 16, 32)                 \
     X(5, 512, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 16, 32)                \
     X(1, 1024, 4, 128, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 3, 11, 32, 32)            \

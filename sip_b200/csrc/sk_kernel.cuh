@@ -173,9 +173,11 @@ struct SkCfg {
 
     static_assert(span(NP) == N, "radices must multiply to N");
     static_assert(!(TW4 && OP != OP_C2C && OP != OP_PC), "cross twiddles are C2C / pulse only");
-    static_assert(!MPAIR || ((OP == OP_R2C_HALF || OP == OP_C2R_HALF || OP == OP_R2C_PAIR || OP == OP_C2R_PAIR) &&
-                             MODE == SK_ROWS && NP >= 2),
-                  "mirrored butterfly pairs: real rows of two or more passes");
+    static_assert(!MPAIR || ((((OP == OP_R2C_HALF || OP == OP_C2R_HALF || OP == OP_R2C_PAIR || OP == OP_C2R_PAIR) &&
+                               MODE == SK_ROWS) ||
+                              (OP == OP_R2C_4B && MODE == SK_ROWS_T)) &&
+                             NP >= 2),
+                  "mirrored butterfly pairs: real rows, or mirrored four-step rows, of two or more passes");
     static_assert(!MPAIR || (OP != OP_R2C_HALF && OP != OP_R2C_PAIR) || SIGN < 0,
                   "R2C tiles run the forward transform");
     static_assert(!MPAIR || (OP != OP_C2R_HALF && OP != OP_C2R_PAIR) || SIGN > 0,
@@ -656,7 +658,7 @@ struct SkPass {
 
 template <class K>
 constexpr bool sk_last_to_smem() {
-    return ((K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR) && !K::MPAIR) || K::OP == OP_R2C_4B || K::OP == OP_PC;
+    return ((K::OP == OP_R2C_HALF || K::OP == OP_R2C_PAIR || K::OP == OP_R2C_4B) && !K::MPAIR) || K::OP == OP_PC;
 }
 
 // R2C value X[k] from Z[k] and Z[M-k] (formula of tile_io.cuh
@@ -854,6 +856,89 @@ SIP_HD void sk_pair_last_r2c(int tid, const TileArgs& a, const TileCtx& c, const
             // X[M - k] belongs to this thread when the mirror is another
             // butterfly; for u = 0 only X[M] (r = 0) is not stored as some X[k]
             if (mirror || (u == 0 && r == 0)) out[M - k] = maybe_conj(y, cj);
+        });
+    }
+}
+
+// Last pass of an R2C_4B tile (pass B of a real four-step: rows k1 = i0 + q
+// in slots [0, H), their mirror rows N1 - k1 in slots [H, 2H)), post-process
+// fused, output to global memory.  With NR = N2 / R, element r of butterfly
+// j of row k1 is bin k2 = j + r NR, output index kk = k1 + N1 k2, whose
+// mirror M - kk = (N1 - k1) + N1 (N2 - 1 - k2) is element R - 1 - r of
+// butterfly NR - 1 - j of row N1 - k1.  One thread takes the unit (q, j):
+// butterfly j of slot q and butterfly NR - 1 - j of slot H + q, and stores
+// X[kk] and X[M - kk] for its R elements.  The two rows that are their own
+// mirror take the partner butterfly from their own slot and store X[kk]
+// only (the mirror bin is another unit's X[kk']): k1 = N1 / 2 (butterfly
+// NR - 1 - j, element R - 1 - r) and k1 = 0 (bin N2 - k2: butterfly NR - j,
+// element R - 1 - r, or for j = 0 element R - r of butterfly 0; the unit
+// j = 0 also stores X[M]).  W_{2M}^{kk} = W_{2M}^{k1 + N1 j} W_{2R}^r: one
+// split-table twiddle per unit times compile-time constants.
+template <class K>
+SIP_HD void sk_pair_last_r2c_4b(int tid, const TileArgs& a, const TileCtx& c, const float2* buf) {
+    constexpr int PASS = K::NP - 1;
+    constexpr int R = K::radix(PASS);
+    constexpr int N2 = K::N;
+    constexpr int NR = N2 / R;
+    constexpr int H = K::H;
+    constexpr int TOTAL = H * NR;
+    constexpr int S = (TOTAL + K::T - 1) / K::T;
+    static_assert(K::span(PASS) == NR, "the last pass spans N / R");
+    const int N1 = a.n_other;
+    const long long M = (long long)N1 * N2;
+    const bool cj = (a.flags & TF_CONJ_OUT) != 0;
+    const bool sc = (a.flags & TF_SCALE) != 0;
+    float2* x = static_cast<float2*>(a.dst) + (c.out_base - c.i0);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) break;
+        const int q = f % H;  // consecutive threads: adjacent rows, so stores run along k1
+        const int j = f / H;
+        if (q >= c.cnt) continue;
+        const int k1 = c.i0 + q;
+        const bool row0 = k1 == 0, half = 2 * k1 == N1, self = row0 || half;
+        const int jb = row0 ? (NR - j) % NR : NR - 1 - j;
+        const float2* ra = buf + q * K::LD;
+        const float2* rb = buf + (self ? q : H + q) * K::LD;
+        float2 A[R], B[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) A[r] = ra[K::idx(j + r * NR)];
+        if (j != 0) {
+            float2 w[R];
+            sk_pass_twiddles<K, PASS>(a, c, j, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) A[r] = c_tw<K::SIGN>(A[r], w[r]);
+        }
+        dft<R, K::SIGN>(A);
+#pragma unroll
+        for (int r = 0; r < R; ++r) B[r] = rb[K::idx(jb + r * NR)];
+        if (jb != 0) {
+            float2 w[R];
+            sk_pass_twiddles<K, PASS>(a, c, jb, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) B[r] = c_tw<K::SIGN>(B[r], w[r]);
+        }
+        dft<R, K::SIGN>(B);
+        const float2 w0 = cross_tw(a, k1 + (long long)N1 * j);  // W_{2M}^{k1 + N1 j}
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            const long long kk = k1 + (long long)N1 * (j + r * NR);
+            const float2 z = A[r];
+            const float2 zm = (row0 && j == 0) ? A[(R - r) % R] : B[R - 1 - r];
+            const float2 w2 = tw_const<2 * R, r, -1>(w0);  // W_{2M}^{kk}
+            const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            const float2 t = c_mul(w2, od);
+            float2 xk = c_add(ev, t);
+            float2 xm = make_float2(ev.x - t.x, t.y - ev.y);  // X[M - kk]; X[M] for kk = 0
+            if (sc) {
+                xk = c_scale(xk, a.scale);
+                xm = c_scale(xm, a.scale);
+            }
+            x[kk] = maybe_conj(xk, cj);
+            if (!self) x[M - kk] = maybe_conj(xm, cj);
+            if (row0 && j == 0 && r == 0) x[M] = maybe_conj(xm, cj);
         });
     }
 }
@@ -1164,6 +1249,8 @@ __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx
         sk_pair_last_r2c<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && K::OP == OP_R2C_PAIR && SP::LAST) {
         sk_pair_last_r2c_rows<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_R2C_4B && SP::LAST) {
+        sk_pair_last_r2c_4b<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
         using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
         typename PP::Regs rg;

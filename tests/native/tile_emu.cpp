@@ -126,6 +126,8 @@ void emu_sk_passes(const TileArgs& a, const TileCtx& c, float2* buf) {
         for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && K::OP == OP_R2C_PAIR && SP::LAST) {
         for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c_rows<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_R2C_4B && SP::LAST) {
+        for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c_4b<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
         using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
         std::vector<typename PP::Regs> regs(K::T);
