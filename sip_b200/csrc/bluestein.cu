@@ -75,11 +75,12 @@ cudaError_t bluestein_prepare() {
 }
 
 cudaError_t bluestein_pre(const BluesteinArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_blue_pre, grid2(a.m, a.rows), dim3(kBlueBlock), 0, stream, a);
+    return launch_pdl(k_blue_pre, grid2(a.m, a.rows), dim3(kBlueBlock), 0, stream, a.m * a.rows, a);
 }
 
 cudaError_t bluestein_post(const BluesteinArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_blue_post, grid2(blue_out_count(a), a.rows), dim3(kBlueBlock), 0, stream, a);
+    return launch_pdl(k_blue_post, grid2(blue_out_count(a), a.rows), dim3(kBlueBlock), 0, stream,
+                      blue_out_count(a) * a.rows, a);
 }
 
 cudaError_t gen_blue_b(float2* out, long long n, long long m, int sign, cudaStream_t stream) {

@@ -49,6 +49,9 @@ namespace {
 thread_local int g_compute_mode = kComputeFp32;
 thread_local int g_hint_p = 0, g_hint_e = 0, g_hint_generic = 0, g_hint_order = 0, g_hint_real_fused = 0,
                  g_hint_variant = -1, g_hint_jit = 0;
+// Column length the next four-step split must use (0: the balanced split);
+// set by a caller that needs the passes of a particular split.
+thread_local int g_split_n1 = 0;
 }  // namespace
 
 // ------------------------------------------------------------ radices
@@ -350,10 +353,11 @@ bool four_step_split(long long n, int* n1, int* n2) {
         best1 = (int)a;  // ascending a: the last hit is the most balanced
     }
     if (best1 == 0) return false;
-    // SIP_FFT_SPLIT_N1 (tuning sweeps): the column length, when it divides n
-    // into two lengths that fit a tile
-    if (const char* e = std::getenv("SIP_FFT_SPLIT_N1")) {
-        const long long a = std::atoll(e);
+    // SIP_FFT_SPLIT_N1 (tuning sweeps) or a caller's choice: the column
+    // length, when it divides n into two lengths that fit a tile
+    const char* env = std::getenv("SIP_FFT_SPLIT_N1");
+    if (g_split_n1 > 0 || env != nullptr) {
+        const long long a = g_split_n1 > 0 ? g_split_n1 : std::atoll(env);
         if (a >= 2 && n % a == 0 && a <= kMaxTileN && n / a <= kMaxTileN && factorizable((int)a, 32) &&
             factorizable((int)(n / a), 32))
             best1 = (int)a;
@@ -992,10 +996,26 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     const bool split = four_step_split(m, &n1, &n2);
     const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr || g_hint_generic;
     const bool fuse = g_hint_real_fused == 1 || (g_hint_real_fused == 0 && r2c);
+    // R2C without a variant hint: the split whose pass B has the post-process
+    // on mirrored butterfly pairs (rows of 512 for m = 2^19: 1.36 ms for
+    // 2^20 x 256 against 1.46 with the 512 x 1024 split's pass B, which
+    // holds 16 rows of 1024 in one CTA per SM)
+    const SkEntry* pair_b = nullptr;
+    if (split && !generic_only && fuse && r2c && g_hint_variant < 0 && !std::getenv("SIP_FFT_SPLIT_N1")) {
+        for (const int b : {n1, n2}) {  // shorter rows first: smaller tiles, more CTAs per SM
+            const SkEntry* e = sk_find_flags(OP_R2C_4B, SK_ROWS_T, -1, false, b, SK_MIRROR_PAIR);
+            if (e != nullptr && sk_find(OP_C2C, SK_COLS, -1, true, (int)(m / b)) != nullptr) {
+                pair_b = e;
+                n1 = (int)(m / b);
+                n2 = b;
+                break;
+            }
+        }
+    }
     if (split && !generic_only && fuse) {
         const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1)
                                 : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1, g_hint_variant);
-        const SkEntry* eb = r2c ? sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2, g_hint_variant)
+        const SkEntry* eb = r2c ? (pair_b != nullptr ? pair_b : sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2, g_hint_variant))
                                 : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
         if (ea != nullptr && eb != nullptr) {
             if (r2c) {
@@ -1003,7 +1023,14 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
                 o.sign = -1;
                 o.src = Loc::In;
                 o.dst = Loc::Out;  // replaced: pass B below
-                add_c2c_1d(plan, m, rows, o);
+                g_split_n1 = n1;   // pass A of this split
+                try {
+                    add_c2c_1d(plan, m, rows, o);
+                } catch (...) {
+                    g_split_n1 = 0;
+                    throw;
+                }
+                g_split_n1 = 0;
                 plan.steps.pop_back();  // keep pass A (column FFTs + cross twiddles) only
                 AxisIO io;
                 io.in_odist = m;

@@ -131,27 +131,27 @@ dim3 grid_for(long long per_row, long long rows, int block) {
 }  // namespace
 
 cudaError_t real_post(const RealPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_real_post, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_real_post, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a.m * a.rows, a);
 }
 
 cudaError_t real_pre(const RealPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_real_pre, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_real_pre, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a.m * a.rows, a);
 }
 
 cudaError_t pair_pack(const PairPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_pair_pack, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_pair_pack, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a.n * a.rows, a);
 }
 
 cudaError_t pair_separate(const PairPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_pair_separate, grid_for(a.n / 2 + 1, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_pair_separate, grid_for(a.n / 2 + 1, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a.n * a.rows, a);
 }
 
 cudaError_t pair_combine(const PairPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_pair_combine, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_pair_combine, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a.n * a.rows, a);
 }
 
 cudaError_t pair_split(const PairPassArgs& a, cudaStream_t stream) {
-    return launch_pdl(k_pair_split, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a);
+    return launch_pdl(k_pair_split, grid_for(a.n, (a.rows + 1) / 2, 256), dim3(256), 0, stream, a.n * a.rows, a);
 }
 
 }  // namespace sipfft

@@ -36,22 +36,8 @@ SIP_HD constexpr int sk_index(int n, int r0) { return r0 % 2 == 0 ? n + n / sk_p
 SIP_HD constexpr int sk_pitch(int n, int r0) {
     return ((sk_index(n - 1, r0) + 1) & 1) ? sk_index(n - 1, r0) + 1 : sk_index(n - 1, r0) + 2;
 }
-// Bits of a configuration's TWB parameter (SkCfg):
-//   SK_TW_BASIS     pass twiddles from the basis table (fewer loads, one
-//                   product more) instead of the full Stockham table;
-//   SK_TW_SMEM      the pass twiddle table and the real pre/post-process
-//                   twiddles are copied to shared memory once per
-//                   persistent CTA and read from there;
-//   SK_MIRROR_PAIR  real tiles: the last pass of an R2C (first pass of a
-//                   C2R) gives each thread butterfly u and its mirror
-//                   NR - u, so that the post-process (pre-process) runs on
-//                   registers (sk_pair_last_r2c, SkPairFirstC2R);
-//   SK_SPLIT_PASS0  pass 0 reads the staging buffer and writes the work
-//                   layout into the other buffer, one butterfly (pair) at a
-//                   time instead of all of them across a barrier; the next
-//                   tile is staged after pass 0 (overlapping the later
-//                   passes) instead of before it.
-enum : int { SK_TW_BASIS = 1, SK_TW_SMEM = 2, SK_MIRROR_PAIR = 4, SK_SPLIT_PASS0 = 8 };
+// The TWB bits (SK_TW_BASIS, SK_TW_SMEM, SK_MIRROR_PAIR, SK_SPLIT_PASS0) are
+// defined in sk_modes.h.
 
 SIP_HD constexpr int sk_twcount(int r, bool basis) { return basis ? basis_count(r) : r - 1; }
 // Entries per table row of pass p in shared memory: all L values k of the

@@ -43,6 +43,12 @@ const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant)
     return first;
 }
 
+const SkEntry* sk_find_flags(int op, int mode, int sign, bool tw4, int n, int flags) {
+    for (const SkEntry& x : sk_registry())
+        if (x.op == op && x.mode == mode && x.sign == sign && x.tw4 == tw4 && x.n == n && (x.flags & flags) == flags)
+            return &x;
+    return nullptr;
+}
 const SkEntry* sk_find_wider(const SkEntry* e) {
     for (const SkEntry& x : sk_registry())
         if (x.op == e->op && x.mode == e->mode && x.sign == e->sign && x.tw4 == e->tw4 && x.n == e->n &&

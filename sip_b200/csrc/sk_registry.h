@@ -27,6 +27,10 @@ struct SkEntry {
 // not compiled; nullptr when no entry is.
 const SkEntry* sk_find(int op, int mode, int sign, bool tw4, int n, int variant = 0);
 
+// The first compiled entry for (op, mode, sign, tw4, n) whose TWB bits
+// include all of `flags`; nullptr if none.
+const SkEntry* sk_find_flags(int op, int mode, int sign, bool tw4, int n, int flags);
+
 // The first compiled variant of `e`'s kernel (same op, mode, sign, tw4, n
 // and transforms per tile) with more threads per tile; nullptr if none.
 const SkEntry* sk_find_wider(const SkEntry* e);

@@ -48,7 +48,8 @@ bool pdl_enabled() {
 }
 
 // Both kernel families wait for the previous kernel of the stream before
-// touching global memory (grid_dep_wait), so both launch with PDL.
+// touching global memory (grid_dep_wait), so both launch with PDL when the
+// launch is one wave of tiles.
 cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStream_t stream) {
     TileArgs a = L.args;
     a.src = src;
@@ -58,7 +59,8 @@ cudaError_t tile_launch(const TileLaunch& L, const void* src, void* dst, cudaStr
     if (fn == nullptr) return cudaErrorInvalidValue;
     void* params[] = {&a};
     cudaLaunchAttribute attr;
-    const cudaLaunchConfig_t cfg = pdl_config(dim3(L.grid), dim3(L.block), (size_t)L.smem_bytes, stream, &attr);
+    const cudaLaunchConfig_t cfg =
+        pdl_config(dim3(L.grid), dim3(L.block), (size_t)L.smem_bytes, stream, &attr, a.ntiles <= L.grid);
     return cudaLaunchKernelExC(&cfg, fn, params);
 }
 
