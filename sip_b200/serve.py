@@ -10,7 +10,7 @@ overlaps on the device.  Plans, twiddle tables and filter spectra stay
 resident; each request's input, output and workspace come from one arena
 sized to the budget.
 
-Two executors share the scheduler:
+Three executors share the scheduler:
   * `QueueExecutor`: the library's persistent work queue (sipFftBatch*), one
     launch per pass index for the whole group, replayed from a captured CUDA
     graph, with the fused pulse-compression kernels; one plan per length
@@ -239,6 +239,11 @@ class Scheduler:
             if not progressed:
                 nxt = pending[0].arrival - now if pending else 0.0
                 self.sleep(max(0.0, min(nxt, 20e-6)) if inflight or not pending else max(0.0, min(nxt, 1e-3)))
+        scale = getattr(ex, "clock_scale", None)
+        if callable(scale):  # device completion times onto the host clock
+            s = scale()
+            for r in stats.requests:
+                r.done *= s
         stats.makespan = max(r.done for r in stats.requests) - min(r.arrival for r in stats.requests)
         return stats
 
@@ -331,14 +336,33 @@ class _GpuBase:
         xv[:, r.delay:r.delay + L] += self.chirp(r.n)
 
     def start(self) -> None:
+        # The device is idle when the start event is recorded, so the event
+        # runs within microseconds of the record call: the host clock is
+        # read right before it, and host and device times share one origin
+        # (device times are at most those microseconds late).
         self.torch.cuda.synchronize(self.dev)
         self.t0_event = self.torch.cuda.Event(enable_timing=True)
+        self.t0_host = time.perf_counter()
         self.t0_event.record(self.streams[0])
         self.t0_event.synchronize()
-        self.t0_host = time.perf_counter()
 
     def now(self) -> float:
         return time.perf_counter() - self.t0_host
+
+    def clock_scale(self) -> float:
+        """Host seconds per device-timer second over the run: a second pair
+        of host and device stamps at its end (the two clocks drift apart by
+        about ten microseconds per second, which over a run of tens of
+        seconds exceeds the latencies being measured).  Device completion
+        times are multiplied by it."""
+        torch = self.torch
+        torch.cuda.synchronize(self.dev)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t1_host = time.perf_counter()
+        t1.record(self.streams[0])
+        t1.synchronize()
+        dev = self.t0_event.elapsed_time(t1) / 1e3
+        return (t1_host - self.t0_host) / dev if dev > 0 else 1.0
 
     def poll(self, token):
         ev = token
