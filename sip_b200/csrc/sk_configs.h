@@ -92,6 +92,9 @@
        rows of 512 (split 1024 x 512) and of 1024 (split 512 x 1024) */      \
     X(4, 512, 16, 256, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 2, 5, 32, 16)             \
     X(5, 1024, 16, 512, OP_R2C_4B, SK_ROWS_T, -1, false, 1, 1, 5, 16, 4, 16)         \
+    /* C2R pre-process + pass A on mirrored butterfly pairs (TWB 5) */       \
+    X(6, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 2, 5, 16, 32)                \
+    X(7, 512, 16, 256, OP_C2R_4A, SK_COLS, 1, false, 1, 1, 5, 16, 32)                \
     X(4, 512, 16, 256, OP_C2C, SK_ROWS_T, 1, false, 1, 3, 1, 16, 32)                 \
     X(5, 512, 16, 256, OP_C2C, SK_ROWS_T, -1, false, 1, 3, 1, 16, 32)                \
     X(1, 1024, 4, 128, OP_R2C_4B, SK_ROWS_T, -1, false, 2, 3, 11, 32, 32)            \

@@ -161,7 +161,7 @@ struct SkCfg {
     static_assert(!(TW4 && OP != OP_C2C && OP != OP_PC), "cross twiddles are C2C / pulse only");
     static_assert(!MPAIR || ((((OP == OP_R2C_HALF || OP == OP_C2R_HALF || OP == OP_R2C_PAIR || OP == OP_C2R_PAIR) &&
                                MODE == SK_ROWS) ||
-                              (OP == OP_R2C_4B && MODE == SK_ROWS_T)) &&
+                              (OP == OP_R2C_4B && MODE == SK_ROWS_T) || (OP == OP_C2R_4A && MODE == SK_COLS)) &&
                              NP >= 2),
                   "mirrored butterfly pairs: real rows, or mirrored four-step rows, of two or more passes");
     static_assert(!MPAIR || (OP != OP_R2C_HALF && OP != OP_R2C_PAIR) || SIGN < 0,
@@ -1086,6 +1086,102 @@ SIP_HD void sk_pair_last_r2c_rows(int tid, const TileArgs& a, const TileCtx& c, 
     }
 }
 
+// Pass 0 of a C2R_4A tile (pass A of a real four-step: columns n2 = i0 + q
+// in slots [0, H), their mirror columns N2 - n2 in slots [H, 2H)), the
+// pre-process fused on mirrored butterfly pairs.  Bin n = n1 N2 + n2 of the
+// half spectrum pairs with M - n = (N1 - 1 - n1) N2 + (N2 - n2): with NR =
+// N1 / R, element r of butterfly j of column n2 (row n1 = j + r NR) pairs
+// with element R - 1 - r of butterfly NR - 1 - j of the mirror column.  One
+// thread takes the unit (q, j), reads both bins of each pair once, and
+// forms Z[n] = E + i W_{2M}^{+n} D and Z[M - n] from them with one
+// split-table twiddle W_{2M}^{j N2 + n2} per unit times the constants
+// W_{2R}^r, then runs both butterflies.  The columns that are their own
+// mirror (n2 = 0: rows n1 and N1 - n1, with X[M] for n1 = 0; n2 = N2 / 2:
+// rows n1 and N1 - 1 - n1) read the partner bin from their own slot and
+// form Z[n] only: every butterfly of such a column is some unit's first.
+template <class K>
+struct SkPairFirstC2R4A {
+    static constexpr int R = K::radix(0);
+    static constexpr int N1 = K::N;
+    static constexpr int NR = N1 / R;
+    static constexpr int H = K::H;
+    static constexpr int TOTAL = H * NR;
+    static constexpr int S = (TOTAL + K::T - 1) / K::T;
+    static_assert(K::span(1) == R, "pass 0 has span 1");
+    struct Regs {
+        float2 a[S][R], b[S][R];
+    };
+
+    SIP_HD static bool unit(int tid, int s, const TileCtx& c, int& q, int& j) {
+        const int f = tid + s * K::T;
+        if (TOTAL % K::T != 0 && f >= TOTAL) return false;
+        q = f % H;  // consecutive threads: adjacent columns (contiguous in the staged rows)
+        j = f / H;
+        return q < c.cnt;
+    }
+
+    SIP_HD static bool read_slot(int tid, int s, const TileArgs& a, const TileCtx& c, const float2* stage,
+                                 float2 (&A)[R], float2 (&B)[R]) {
+        int q, j;
+        if (!unit(tid, s, c, q, j)) return false;
+        const int n2c = a.n_other;
+        const int col = c.i0 + q;
+        const bool col0 = col == 0, half = 2 * col == n2c, self = col0 || half;
+        const bool cj = (a.flags & TF_CONJ_IN) != 0;
+        const float2 w0 = cross_tw(a, (long long)j * n2c + col);  // W_{2M}^{j N2 + n2}
+        sk_static_for<0, R>([&](auto ic) {
+            constexpr int r = decltype(ic)::value;
+            const int n1 = j + r * NR;
+            const float2 x = maybe_conj(stage[n1 * K::P + q], cj);
+            if (col0 && n1 == 0) {  // Z[0] from the real parts of X[0] and X[M]
+                const float2* xrow = static_cast<const float2*>(a.src) + (c.in_base - c.i0);
+                const float ny = SIP_LDG(xrow + (long long)N1 * n2c).x;
+                A[r] = make_float2(0.5f * (x.x + ny), 0.5f * (x.x - ny));
+                return;
+            }
+            const int prow = col0 ? N1 - n1 : N1 - 1 - n1;
+            const float2 y = maybe_conj(stage[prow * K::P + (self ? q : H + q)], cj);
+            const float2 w = tw_const<2 * R, r, -1>(w0);  // W_{2M}^{n}
+            const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+            const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));
+            const float2 od = c_mulc(d, w);
+            A[r] = make_float2(e.x - od.y, e.y + od.x);           // Z[n]
+            B[R - 1 - r] = make_float2(e.x + od.y, od.x - e.y);   // Z[M - n]
+        });
+        dft<R, K::SIGN>(A);
+        if (!self) dft<R, K::SIGN>(B);
+        return true;
+    }
+
+    // Pass 0 has span 1: butterfly j writes element r to j R + r.
+    SIP_HD static void write_slot(int tid, int s, const TileArgs& a, const TileCtx& c, float2* buf,
+                                  const float2 (&A)[R], const float2 (&B)[R]) {
+        int q, j;
+        if (!unit(tid, s, c, q, j)) return;
+        const int col = c.i0 + q;
+        float2* ra = buf + q * K::LD;
+#pragma unroll
+        for (int r = 0; r < R; ++r) ra[K::idx(j * R + r)] = A[r];
+        if (col != 0 && 2 * col != a.n_other) {
+            float2* rb = buf + (H + q) * K::LD;
+            const int jb = NR - 1 - j;
+#pragma unroll
+            for (int r = 0; r < R; ++r) rb[K::idx(jb * R + r)] = B[r];
+        }
+    }
+
+    SIP_HD static void read(int tid, const TileArgs& a, const TileCtx& c, const float2* stage, Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) read_slot(tid, s, a, c, stage, rg.a[s], rg.b[s]);
+    }
+
+    SIP_HD static void write_smem(int tid, const TileArgs& a, const TileCtx& c, float2* buf, const Regs& rg) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) write_slot(tid, s, a, c, buf, rg.a[s], rg.b[s]);
+    }
+};
+
+
 // First pass of a C2R_PAIR tile from the staged spectra of real rows 2q and
 // 2q + 1 (N/2 + 1 bins each): Z[n] = Xa[n] + i Xb[n] with the Hermitian
 // halves, every staged bin read once (for bin m and its mirror N - m).
@@ -1237,6 +1333,14 @@ __device__ __forceinline__ void sk_run(int tid, const TileArgs& a, const TileCtx
         sk_pair_last_r2c_rows<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && K::OP == OP_R2C_4B && SP::LAST) {
         sk_pair_last_r2c_4b<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_C2R_4A && PASS == 0) {
+        using PP = SkPairFirstC2R4A<K>;
+        typename PP::Regs rg;
+        PP::read(tid, a, c, buf, rg);
+        __syncthreads();
+        PP::write_smem(tid, a, c, buf, rg);
+        __syncthreads();
+        sk_run<K, 1>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
         using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
         typename PP::Regs rg;

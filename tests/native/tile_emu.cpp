@@ -128,6 +128,12 @@ void emu_sk_passes(const TileArgs& a, const TileCtx& c, float2* buf) {
         for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c_rows<K>(tid, a, c, buf);
     } else if constexpr (K::MPAIR && K::OP == OP_R2C_4B && SP::LAST) {
         for (int tid = 0; tid < K::T; ++tid) sk_pair_last_r2c_4b<K>(tid, a, c, buf);
+    } else if constexpr (K::MPAIR && K::OP == OP_C2R_4A && PASS == 0) {
+        using PP = SkPairFirstC2R4A<K>;
+        std::vector<typename PP::Regs> regs(K::T);
+        for (int tid = 0; tid < K::T; ++tid) PP::read(tid, a, c, buf, regs[tid]);
+        for (int tid = 0; tid < K::T; ++tid) PP::write_smem(tid, a, c, buf, regs[tid]);
+        emu_sk_passes<K, 1>(a, c, buf);
     } else if constexpr (K::MPAIR && (K::OP == OP_C2R_HALF || K::OP == OP_C2R_PAIR) && PASS == 0) {
         using PP = typename SkPick<K::OP == OP_C2R_HALF, SkPairFirstC2R<K>, SkPairFirstC2RRows<K>>::type;
         std::vector<typename PP::Regs> regs(K::T);
