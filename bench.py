@@ -247,7 +247,7 @@ def precision_form(torch, dev, stream, steps: int, warmup: int) -> dict:
     return out
 
 
-def other_configs(torch, dev, stream, steps: int = 10, warmup: int = 3) -> dict:
+def other_configs(torch, dev, stream, steps: int = 100, warmup: int = 10) -> dict:
     """The reference's other benchmark configurations, forward and inverse,
     device-resident, CUDA events: 1D C2C N=4096 x 256 (16.8 MB, so 12
     rotating buffer pairs keep every timed exec's data out of L2), 2D C2C

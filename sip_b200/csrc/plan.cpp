@@ -1075,6 +1075,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
                 Step sb = make_tile_step(OP_C2C, 1, n2, n2, true, b, TF_SCALE, 0,
                                          "four-step B n=" + std::to_string(m) + " n2=" + std::to_string(n2));
                 sb.L.args.scale = 2.0f;
+                sb.batch_dim = 2;  // the batch rows are the outer index
                 sb.src = Loc::Ws;
                 sb.dst = Loc::Out;
                 plan.steps.push_back(sb);

@@ -367,3 +367,14 @@ def test_rows_exec_checks(sip_lib, handle):
     assert plan1d(sip_lib, h3, 100003, C2C, F, 2) == OK   # prime: Bluestein steps
     assert sip_lib.sipFftExecRawRows(h3, 1, x, y, None) == NOTSUP
     sip_lib.asdFftDestroy(h3)
+
+
+@pytest.mark.parametrize("t,n", [(R2C, 1 << 20), (C2R, 1 << 20), (C2C, 65536), (R2C, 6000), (C2R, 1000),
+                                 (C2C, 4096)])
+def test_rows_exec_supported_for_1d_plans(sip_lib, handle, t, n):
+    """Every 1-D plan of a benchmark length can run on its first rows: the
+    row-limited exec passes its plan checks and stops only at the missing
+    device (or workspace), not with API_NOT_SUPPORT."""
+    assert plan1d(sip_lib, handle, n, t, F if t != C2R else L.ASCEND_FFT_INVERSE, 4) == OK
+    rc = sip_lib.sipFftExecRawRows(handle, 2, ctypes.c_void_p(0x10000), ctypes.c_void_p(0x40000000), None)
+    assert rc == INTERNAL, rc
