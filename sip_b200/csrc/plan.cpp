@@ -987,6 +987,10 @@ void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
 // is slower than a separate pre-process pass plus the plain four-step
 // (2^20 x 256 rows: 2.12 ms fused, 1.74 ms unfused).  The real-fused planner
 // hint selects either form for both directions.
+// The fused C2R pass A on mirrored butterfly pairs as the default C2R form
+// (else a variant under the real-fused and variant hints).
+constexpr bool kC2RPairDefault = false;
+
 void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     if (n % 2 != 0)
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "odd real length " + std::to_string(n) + " above one tile");
@@ -998,7 +1002,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     // C2R without a variant or real-fused hint: the fused pass A when its
     // pre-process runs on mirrored butterfly pairs (each bin pair read once)
     const SkEntry* pair_a = nullptr;
-    if (split && !generic_only && !r2c && g_hint_real_fused == 0 && g_hint_variant < 0 &&
+    if (kC2RPairDefault && split && !generic_only && !r2c && g_hint_real_fused == 0 && g_hint_variant < 0 &&
         sk_find(OP_C2C, SK_ROWS_T, 1, false, n2) != nullptr)
         pair_a = sk_find_flags(OP_C2R_4A, SK_COLS, 1, false, n1, SK_MIRROR_PAIR);
     const bool fuse = g_hint_real_fused == 1 || (g_hint_real_fused == 0 && (r2c || pair_a != nullptr));

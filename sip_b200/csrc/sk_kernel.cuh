@@ -67,7 +67,8 @@ SIP_HD constexpr int sk_tws_values(int op, int n, const int* rs, int np, int fla
 // Staged input values (complex64 units) per tile.
 SIP_HD constexpr int sk_stage_values(int op, int p, int n) {
     return op == OP_C2R_HALF ? p * (n + 1)
-         : (op == OP_R2C_4B || op == OP_C2R_4A) ? p * n
+         : op == OP_R2C_4B ? p * n
+         : op == OP_C2R_4A ? (p + 2) * n  // sk_c2r4a_at: each row H columns, then a span of H + 2
          : op == OP_C2R_PAIR ? p * (n + 1)
          : p * n;  // R2C pair: 2P rows of N floats = P*N complex slots
 }
@@ -349,25 +350,43 @@ SIP_HD void sk_stage(int tid, const TileArgs& a, const TileCtx& c, float2* stage
 #endif
         }
     } else if constexpr (K::OP == OP_C2R_4A) {
-        // element n1 of columns n2 = i0 + q (slot q) and N2 - n2 (slot H + q);
-        // each thread keeps one slot and walks the rows
-        static_assert(T % K::P == 0, "C2R_4A staging maps threads to slots");
+        // Row n1 of the tile: the H columns i0 .. i0 + H - 1 (one run) and
+        // the span of mirror columns N2 - i0 - H .. N2 - i0 + 1 (one run of
+        // H + 2; of H for i0 = 0, whose mirror of column 0 is column 0
+        // itself), in 16-byte copies when the batch row is 16-byte aligned
+        // (sk_c2r4a_at reads them).  Columns past the tile's count stay
+        // inside the row and are not used.
+        static_assert(K::H % 2 == 0, "mirror spans start on an even column");
+        constexpr int SP = K::P + 2;
         const int n2c = a.n_other;
         const char* xbase = src + (c.in_base - c.i0) * 8;  // X[0] of this batch row
-        const int slot = tid % K::P;
-        const int col = sk_c2r4a_col<K>(a, c.i0, c.cnt, slot);
-        if (col >= 0) {
-            const char* s = xbase + (long long)col * 8;
-            char* d = reinterpret_cast<char*>(stage) + slot * 8;
-            for (int n1 = tid / K::P; n1 < K::N; n1 += T / K::P) {
-#if defined(__CUDA_ARCH__)
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
-                                 (unsigned)__cvta_generic_to_shared(d + n1 * K::P * 8)),
-                             "l"(s + (long long)n1 * n2c * 8));
-#else
-                for (int b = 0; b < 8; ++b) d[n1 * K::P * 8 + b] = s[(long long)n1 * n2c * 8 + b];
-#endif
+        const int g = ((reinterpret_cast<uintptr_t>(xbase) & 15) == 0 && n2c % 2 == 0) ? 16 : 8;
+        const int ms0 = n2c - c.i0 - K::H;
+        const int cf = K::H * 8 / g;
+        const int cm = (c.i0 == 0 ? K::H : K::H + 2) * 8 / g;
+        const int per = cf + cm;
+        for (int ch = tid; ch < K::N * per; ch += T) {
+            const int n1 = ch / per;
+            int k = ch - n1 * per;
+            const char* s;
+            char* d;
+            if (k < cf) {
+                s = xbase + ((long long)n1 * n2c + c.i0) * 8 + k * g;
+                d = reinterpret_cast<char*>(stage) + (n1 * SP) * 8 + k * g;
+            } else {
+                k -= cf;
+                s = xbase + ((long long)n1 * n2c + ms0) * 8 + k * g;
+                d = reinterpret_cast<char*>(stage) + (n1 * SP + K::H) * 8 + k * g;
             }
+#if defined(__CUDA_ARCH__)
+            const unsigned da = (unsigned)__cvta_generic_to_shared(d);
+            if (g == 16)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(da), "l"(s));
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(da), "l"(s));
+#else
+            for (int b = 0; b < g; ++b) d[b] = s[b];
+#endif
         }
     } else if constexpr (K::OP == OP_R2C_PAIR) {
         const int r0 = 2 * c.i0;
@@ -402,6 +421,14 @@ SIP_HD void sk_zero_missing(int tid, const TileArgs& a, const TileCtx& c, float2
     }
 }
 
+// Staged element of row n1 in slot `slot`: columns i0 + q at [0, H), the
+// mirror column N2 - (i0 + q) of slot H + q at 2H - q of the mirror span.
+template <class K>
+SIP_HD float2 sk_c2r4a_at(const float2* stage, int n1, int slot) {
+    const float2* row = stage + n1 * (K::P + 2);
+    return slot < K::H ? row[slot] : row[3 * K::H - slot];
+}
+
 // C2R_4A pass-0 input: Z[k] = E + i W_{2M}^{+k} D, k = n1 N2 + n2, from X[k]
 // and X[M-k] (M = N1 N2; the partner sits in the mirror column, row
 // N1-1-n1, or in the same column for n2 = 0 and n2 = N2/2; X[M] itself is
@@ -413,7 +440,7 @@ SIP_HD float2 sk_c2r4a_input(const TileArgs& a, const TileCtx& c, const float2* 
     if (col < 0) return make_float2(0.f, 0.f);
     const long long M = (long long)K::N * n2c;
     const bool cj = (a.flags & TF_CONJ_IN) != 0;
-    float2 x = maybe_conj(stage[n1 * K::P + slot], cj);
+    float2 x = maybe_conj(sk_c2r4a_at<K>(stage, n1, slot), cj);
     float2 y;
     if (col == 0) {
         if (n1 == 0) {
@@ -421,12 +448,12 @@ SIP_HD float2 sk_c2r4a_input(const TileArgs& a, const TileCtx& c, const float2* 
             const float ny = SIP_LDG(xrow + M).x;
             return make_float2(0.5f * (x.x + ny), 0.5f * (x.x - ny));
         }
-        y = stage[(K::N - n1) * K::P + slot];
+        y = sk_c2r4a_at<K>(stage, K::N - n1, slot);
     } else if (2 * col == n2c) {
-        y = stage[(K::N - 1 - n1) * K::P + slot];
+        y = sk_c2r4a_at<K>(stage, K::N - 1 - n1, slot);
     } else {
         const int ms = slot < K::H ? slot + K::H : slot - K::H;
-        y = stage[(K::N - 1 - n1) * K::P + ms];
+        y = sk_c2r4a_at<K>(stage, K::N - 1 - n1, ms);
     }
     y = maybe_conj(y, cj);
     const long long kk = (long long)n1 * n2c + col;
@@ -1132,7 +1159,7 @@ struct SkPairFirstC2R4A {
         sk_static_for<0, R>([&](auto ic) {
             constexpr int r = decltype(ic)::value;
             const int n1 = j + r * NR;
-            const float2 x = maybe_conj(stage[n1 * K::P + q], cj);
+            const float2 x = maybe_conj(sk_c2r4a_at<K>(stage, n1, q), cj);
             if (col0 && n1 == 0) {  // Z[0] from the real parts of X[0] and X[M]
                 const float2* xrow = static_cast<const float2*>(a.src) + (c.in_base - c.i0);
                 const float ny = SIP_LDG(xrow + (long long)N1 * n2c).x;
@@ -1140,7 +1167,7 @@ struct SkPairFirstC2R4A {
                 return;
             }
             const int prow = col0 ? N1 - n1 : N1 - 1 - n1;
-            const float2 y = maybe_conj(stage[prow * K::P + (self ? q : H + q)], cj);
+            const float2 y = maybe_conj(sk_c2r4a_at<K>(stage, prow, self ? q : H + q), cj);
             const float2 w = tw_const<2 * R, r, -1>(w0);  // W_{2M}^{n}
             const float2 e = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
             const float2 d = make_float2(0.5f * (x.x - y.x), 0.5f * (x.y + y.y));

@@ -234,7 +234,7 @@ def test_partial_overlap_rejected(sip_lib, handle):
     (R2C, [1000], ["r2c half"]),
     (R2C, [2187], ["r2c pair"]),
     (R2C, [1 << 20], ["four-step A", "r2c four-step B + post"]),
-    (C2R, [1 << 20], ["c2r pre + four-step A", "four-step B"]),
+    (C2R, [1 << 20], ["c2r pre", "four-step A", "four-step B"]),
     (C2R, [64, 64], ["c2c axis 0", "c2r half"]),
     # Bluestein up to the largest length (2^27): a convolution of 2^28 in
     # the four-step pulse chain
