@@ -71,6 +71,9 @@
     /* odd real length 2187 = 3^7, two rows per complex FFT (the R2C tile  \
        shape from a run-time compiled sweep: 4 % faster than 2 x 192) */     \
     X(7, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 15, 27, 9, 9)          \
+    /* C2R: one row pair per 128-thread CTA, four CTAs per SM (542 us for  \
+       122741 rows against 573 us with two pairs per 192-thread CTA) */      \
+    X(4, 2187, 1, 128, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 4, 11, 27, 9, 9)           \
     X(0, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 11, 27, 9, 9)           \
     X(3, 2187, 2, 192, OP_C2R_PAIR, SK_ROWS, 1, false, 2, 2, 9, 27, 9, 9)            \
     X(1, 2187, 2, 128, OP_R2C_PAIR, SK_ROWS, -1, false, 2, 3, 1, 27, 9, 9)           \

@@ -467,7 +467,20 @@ class ResidentExecutor(_GpuBase):
         check(L.lib().sipFftJitWait(jit_wait_ms), "run-time kernels")
         self._destroy_plans()
         self._make_plans(lengths)
+        self._first_launches()
         self.launches = 0
+
+    def _first_launches(self) -> None:
+        """One row through every plan: CUDA loads a kernel's module on its
+        first launch (lazy loading), which would otherwise land on the first
+        request of each length.  The rows come from the start of the arena
+        (its contents are not used)."""
+        s = self.streams[0]
+        row = 8 * max(n for _, n in self.plans)
+        for h in self.plans.values():
+            self.check(h.set_stream(s), "stream")
+            self.check(h.exec_rows(1, self.base, self.base + row, self.base + 2 * row), "first launch")
+        s.synchronize()
 
     def _make_plans(self, lengths):
         from .fft import FftHandle
