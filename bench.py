@@ -748,15 +748,17 @@ def run_ours(args) -> None:
                "sample": res["sample"] + " (oracle/stockham.c, the C restatement of the reference's arithmetic)"}
 
     prec = None
-    if rank == 0 and not args.no_precision:
+    # the extra forms run in single-GPU runs only: under torchrun the other
+    # ranks would wait for them at the barrier below, past its timeout
+    if rank == 0 and world == 1 and not args.no_precision:
         prec = precision_form(torch, dev, stream, steps=5, warmup=2)
     others = None
     published = None
-    if rank == 0 and not args.no_other:
+    if rank == 0 and world == 1 and not args.no_other:
         others = other_configs(torch, dev, stream)
         published = published_configs(torch, dev, stream)
     serve = None
-    if rank == 0 and not args.no_serve:
+    if rank == 0 and world == 1 and not args.no_serve:
         try:
             serve = serving(torch, args.serve_requests)
         finally:
