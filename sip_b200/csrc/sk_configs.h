@@ -27,6 +27,15 @@
     /* strided axes of 2D / 3D transforms */                                  \
     X(2, 2048, 8, 512, OP_C2C, SK_COLS, -1, false, 1, 1, 1, 16, 16, 8)               \
     X(3, 2048, 8, 512, OP_C2C, SK_COLS, 1, false, 1, 1, 1, 16, 16, 8)                \
+    /* 256-point column and transposed-row passes: 16 transforms per       \
+       128-thread CTA with a split pass 0 (C2C 65536 x 4096: 1.78 ms against \
+       1.84 with 256-thread CTAs); the 256-thread form is a hint variant */  \
+    X(4, 256, 16, 128, OP_C2C, SK_COLS, -1, false, 2, 3, 9, 16, 16)                  \
+    X(5, 256, 16, 128, OP_C2C, SK_COLS, 1, false, 2, 3, 9, 16, 16)                   \
+    X(6, 256, 16, 128, OP_C2C, SK_COLS, -1, true, 2, 3, 9, 16, 16)                   \
+    X(7, 256, 16, 128, OP_C2C, SK_COLS, 1, true, 2, 3, 9, 16, 16)                    \
+    X(0, 256, 16, 128, OP_C2C, SK_ROWS_T, -1, false, 2, 3, 9, 16, 16)                \
+    X(1, 256, 16, 128, OP_C2C, SK_ROWS_T, 1, false, 2, 3, 9, 16, 16)                 \
     X(4, 256, 16, 256, OP_C2C, SK_COLS, -1, false, 2, 3, 1, 16, 16)                  \
     X(5, 256, 16, 256, OP_C2C, SK_COLS, 1, false, 2, 3, 1, 16, 16)                   \
     /* four-step 65536 = 256 x 256 */                                         \
