@@ -35,43 +35,22 @@ __global__ void k_real_post(const RealPassArgs a) {
     }
 }
 
-// Each thread takes kPreUnroll pairs a grid stride apart and issues all
-// their loads before any arithmetic, so that more reads are in flight per
-// thread.
-constexpr int kPreUnroll = 4;
-
 __global__ void k_real_pre(const RealPassArgs a) {
     grid_dep_wait();
     grid_dep_launch();
     const long long pairs = a.m / 2 + 1;
     const bool cj = a.conj != 0;
-    const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long row = blockIdx.y; row < a.rows; row += gridDim.y) {
         const float2* x = a.src + row * a.in_pitch;
         float2* z = a.dst + row * a.out_pitch;
-        for (long long k0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k0 < pairs;
-             k0 += stride * kPreUnroll) {
-            float2 xv[kPreUnroll], yv[kPreUnroll], w[kPreUnroll];
-#pragma unroll
-            for (int u = 0; u < kPreUnroll; ++u) {
-                const long long k = k0 + u * stride;
-                if (k > 0 && k < a.m - k) {
-                    xv[u] = SIP_LDG(x + k);
-                    yv[u] = SIP_LDG(x + a.m - k);
-                    w[u] = SIP_LDG(a.tw + k);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kPreUnroll; ++u) {
-                const long long k = k0 + u * stride;
-                if (k >= pairs) break;
-                const long long km = a.m - k;
-                if (k > 0 && k < km) {
-                    real_pre_pair_values(xv[u], yv[u], w[u], cj, z + k, z + km);
-                } else {
-                    z[k] = real_pre_elem(x, k, a.m, a.tw, cj);
-                    if (km != k && km < a.m) z[km] = real_pre_elem(x, km, a.m, a.tw, cj);
-                }
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < pairs;
+             k += (long long)gridDim.x * blockDim.x) {
+            const long long km = a.m - k;
+            if (k > 0 && k < km) {
+                real_pre_pair(x, k, a.m, a.tw, cj, z + k, z + km);
+            } else {
+                z[k] = real_pre_elem(x, k, a.m, a.tw, cj);
+                if (km != k && km < a.m) z[km] = real_pre_elem(x, km, a.m, a.tw, cj);
             }
         }
     }
@@ -156,8 +135,7 @@ cudaError_t real_post(const RealPassArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t real_pre(const RealPassArgs& a, cudaStream_t stream) {
-    const long long per = (a.m / 2 + 1 + kPreUnroll - 1) / kPreUnroll;  // pairs per row over the unroll
-    return launch_pdl(k_real_pre, grid_for(per, a.rows, 256), dim3(256), 0, stream, a.m * a.rows, a);
+    return launch_pdl(k_real_pre, grid_for(a.m / 2 + 1, a.rows, 256), dim3(256), 0, stream, a.m * a.rows, a);
 }
 
 cudaError_t pair_pack(const PairPassArgs& a, cudaStream_t stream) {

@@ -64,8 +64,9 @@ SIP_HD void real_post_pair(const float2* z, long long k, long long m, const floa
 // with Z[k] = e + i W^{-k} d (e, d from x[k] and conj x[m - k]), the mirror
 // is Z[m - k] = conj(e) + conj(i W^{-k} d) (its e is conj(e), its d is
 // -conj(d), and W^{-(m-k)} = -conj(W^{-k})).
-// Z[k] and Z[m - k] from the loaded X[k], X[m - k] and W_{2m}^k.
-SIP_HD void real_pre_pair_values(float2 xv, float2 yv, float2 w, bool conj, float2* zk, float2* zmk) {
+SIP_HD void real_pre_pair(const float2* x, long long k, long long m, const float2* tw, bool conj, float2* zk,
+                          float2* zmk) {
+    float2 xv = SIP_LDG(x + k), yv = SIP_LDG(x + m - k);
     if (conj) {
         xv.y = -xv.y;
         yv.y = -yv.y;
@@ -73,14 +74,9 @@ SIP_HD void real_pre_pair_values(float2 xv, float2 yv, float2 w, bool conj, floa
     const float2 b = make_float2(yv.x, -yv.y);
     const float2 e = make_float2(0.5f * (xv.x + b.x), 0.5f * (xv.y + b.y));
     const float2 d = make_float2(0.5f * (xv.x - b.x), 0.5f * (xv.y - b.y));
-    const float2 od = c_mulc(d, w);
+    const float2 od = c_mulc(d, SIP_LDG(tw + k));
     *zk = make_float2(e.x - od.y, e.y + od.x);
     *zmk = make_float2(e.x + od.y, -e.y + od.x);
-}
-
-SIP_HD void real_pre_pair(const float2* x, long long k, long long m, const float2* tw, bool conj, float2* zk,
-                          float2* zmk) {
-    real_pre_pair_values(SIP_LDG(x + k), SIP_LDG(x + m - k), SIP_LDG(tw + k), conj, zk, zmk);
 }
 
 // ---------------------------------------- odd real lengths above one tile
