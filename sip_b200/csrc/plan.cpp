@@ -987,10 +987,6 @@ void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
 // is slower than a separate pre-process pass plus the plain four-step
 // (2^20 x 256 rows: 2.12 ms fused, 1.74 ms unfused).  The real-fused planner
 // hint selects either form for both directions.
-// The fused C2R pass A on mirrored butterfly pairs as the default C2R form
-// (else a variant under the real-fused and variant hints).
-constexpr bool kC2RPairDefault = false;
-
 void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     if (n % 2 != 0)
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "odd real length " + std::to_string(n) + " above one tile");
@@ -999,13 +995,10 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     int n1 = 0, n2 = 0;
     const bool split = four_step_split(m, &n1, &n2);
     const bool generic_only = std::getenv("SIP_FFT_GENERIC_ONLY") != nullptr || g_hint_generic;
-    // C2R without a variant or real-fused hint: the fused pass A when its
-    // pre-process runs on mirrored butterfly pairs (each bin pair read once)
-    const SkEntry* pair_a = nullptr;
-    if (kC2RPairDefault && split && !generic_only && !r2c && g_hint_real_fused == 0 && g_hint_variant < 0 &&
-        sk_find(OP_C2C, SK_ROWS_T, 1, false, n2) != nullptr)
-        pair_a = sk_find_flags(OP_C2R_4A, SK_COLS, 1, false, n1, SK_MIRROR_PAIR);
-    const bool fuse = g_hint_real_fused == 1 || (g_hint_real_fused == 0 && (r2c || pair_a != nullptr));
+    // C2R stays unfused by default: its fused pass A, with the pre-process on
+    // mirrored butterfly pairs too, measured slower (1.38 ms against 0.45 +
+    // 0.60 ms for 2^20 x 256); the real-fused and variant hints select it.
+    const bool fuse = g_hint_real_fused == 1 || (g_hint_real_fused == 0 && r2c);
     // R2C without a variant hint: the split whose pass B has the post-process
     // on mirrored butterfly pairs (rows of 512 for m = 2^19: 1.36 ms for
     // 2^20 x 256 against 1.46 with the 512 x 1024 split's pass B, which
@@ -1024,7 +1017,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     }
     if (split && !generic_only && fuse) {
         const SkEntry* ea = r2c ? sk_find(OP_C2C, SK_COLS, -1, true, n1)
-                                : (pair_a != nullptr ? pair_a : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1, g_hint_variant));
+                                : sk_find(OP_C2R_4A, SK_COLS, 1, false, n1, g_hint_variant);
         const SkEntry* eb = r2c ? (pair_b != nullptr ? pair_b : sk_find(OP_R2C_4B, SK_ROWS_T, -1, false, n2, g_hint_variant))
                                 : sk_find(OP_C2C, SK_ROWS_T, 1, false, n2);
         if (ea != nullptr && eb != nullptr) {

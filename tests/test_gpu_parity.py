@@ -240,3 +240,50 @@ def test_cluster_four_step(cuda, n, batch, direction, monkeypatch):
     h.destroy()
     out0 = gpu_run(cuda, O.C2C, direction, [n], batch, x)
     assert O.rel_l2(out0, want) <= REL_L2_TOL
+
+
+# (type, direction, planner hints, step holding the mirrored pairs, its length)
+MIRRORED_FORMS = [
+    (O.R2C, O.FORWARD, {}, 1, 512),             # default: 1024 x 512 split, pass B on pairs
+    (O.R2C, O.INVERSE, {}, 1, 512),
+    (O.R2C, O.FORWARD, {6: 2}, 1, 1024),        # 512 x 1024 split, pass B on pairs (variant)
+    (O.C2R, O.INVERSE, {5: 1, 6: 1}, 0, 512),   # fused pre-process in pass A on pairs (variant)
+    (O.C2R, O.FORWARD, {5: 1, 6: 1}, 0, 512),
+    (O.C2R, O.INVERSE, {5: 1, 6: 0}, 0, None),  # fused pre-process, element by element (variant)
+]
+
+
+@pytest.mark.parametrize("op,direction,hints,step,n_pair", MIRRORED_FORMS)
+@pytest.mark.parametrize("batch", [1, 5])
+def test_real_four_step_mirrored_forms(cuda, op, direction, hints, step, n_pair, batch):
+    """The real 2^20 four-step forms whose pass B (R2C) or pass A (C2R)
+    handles a row or column together with its mirror: the planner picks the
+    expected kernel (TWB bit 4 where the post- or pre-process runs on
+    mirrored butterfly pairs) and the result matches FP64."""
+    from tests.fftcase import random_input, settle, shapes
+    from sip_b200.fft import FftHandle, check
+
+    torch = cuda
+    n = 1 << 20
+    x = random_input(op, [n], batch, seed=batch + 31 * len(hints))
+    h = FftHandle()
+    for k, v in hints.items():
+        check(h.set_hint(k, v), "hint")
+    check(h.make_plan_1d(n, op, direction, batch), "plan")
+    cfg = h.describe()["steps"][step]["sk_cfg"]
+    if n_pair is None:
+        assert not cfg[8] & 4
+    else:
+        assert cfg[8] & 4 and cfg[0] == n_pair, cfg
+    h.bind_workspace()
+    s = torch.cuda.Stream()
+    check(h.set_stream(s), "stream")
+    _, _, oshape, odt = shapes(op, [n], batch)
+    xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    yt = torch.zeros(oshape, dtype=torch.complex64 if odt == np.complex64 else torch.float32, device="cuda")
+    settle()
+    check((h.exec_r2c if op == O.R2C else h.exec_c2r)(xt, yt), "exec")
+    s.synchronize()
+    err = O.rel_l2(yt.cpu().numpy(), O.fp64(op, direction, x, [n]))
+    h.destroy()
+    assert err <= REL_L2_TOL, f"rel_l2 {err:.3e}"
