@@ -247,9 +247,45 @@ def precision_form(torch, dev, stream, steps: int, warmup: int) -> dict:
     return out
 
 
+def graph_exec_ms(torch, h, xs, ys, stream, steps: int):
+    """Per-exec time of `steps` back-to-back execs (rotating buffers)
+    captured once in a CUDA graph and replayed, the reference's own timing
+    protocol; None when the capture fails."""
+    from sip_b200.fft import check
+
+    nbuf = len(xs)
+    try:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                for i in range(steps):
+                    check(h.exec_raw(xs[i % nbuf].data_ptr(), ys[i % nbuf].data_ptr()), "exec")
+            finally:
+                g.capture_end()
+        for _ in range(2):
+            g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            g.replay()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        del g
+        return ms
+    except Exception as ex:  # capture unsupported: report the stream timing only
+        print(f"graph capture failed: {ex}", file=sys.stderr)
+        torch.cuda.synchronize()
+        return None
+
+
 def other_configs(torch, dev, stream, steps: int = 100, warmup: int = 10) -> dict:
     """The reference's other benchmark configurations, forward and inverse,
-    device-resident, CUDA events: 1D C2C N=4096 x 256 (16.8 MB, so 12
+    device-resident, CUDA events (`ms`: execs launched on the stream back to
+    back; `ms_graph`: the same execs replayed from a CUDA graph, the
+    reference's protocol): 1D C2C N=4096 x 256 (16.8 MB, so 12
     rotating buffer pairs keep every timed exec's data out of L2), 2D C2C
     2048 x 2048 x 8 and 3D C2C 256^3 (one HBM pass per axis).  Inputs
     i.i.d. N(0, 1), seed 20261029 + N; rel-L2 against the FP64 oracle on the
@@ -293,11 +329,12 @@ def other_configs(torch, dev, stream, steps: int = 100, warmup: int = 10) -> dic
             e1.record(stream)
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / steps
+            ms_graph = graph_exec_ms(torch, h, xs, ys, stream, steps)
             check(h.exec_raw(xs[0].data_ptr(), ys[0].data_ptr()), "exec")
             torch.cuda.synchronize()
             x0 = xs[0][:1].cpu().numpy()
             err = O.rel_l2(ys[0][:1].cpu().numpy(), O.fp64(O.C2C, d, x0, sizes))
-            res[dname] = {"ms": round(ms, 4), "passes": passes,
+            res[dname] = {"ms": round(ms, 4), "ms_graph": round(ms_graph, 4) if ms_graph else None, "passes": passes,
                           "gbs_moved": round(16 * elems * passes / (ms * 1e-3) / 1e9, 1),
                           "gbs_algorithmic": round(16 * elems / (ms * 1e-3) / 1e9, 1),
                           "gflops": round(flops / (ms * 1e-3) / 1e9, 1), "rel_l2": float(f"{err:.3e}")}
