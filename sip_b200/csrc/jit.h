@@ -35,8 +35,10 @@ struct JitCfg {
 };
 
 // Host-side configuration for at most `values` values per thread and pass
-// (0: SIP_FFT_JIT_E or 32); no CUDA or NVRTC calls.
-bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out, int values = 0);
+// (0: SIP_FFT_JIT_E or 32), with the radices in the given order (null: the
+// cheapest factorization, largest radix first); no CUDA or NVRTC calls.
+bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transforms, JitCfg* out, int values = 0,
+                   const std::vector<int>* order = nullptr);
 
 // The configuration the planner uses: candidates of sk_jit_choose compiled
 // in turn (32, 16, 48 values per thread) until one has no register spills

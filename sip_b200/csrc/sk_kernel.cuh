@@ -1328,12 +1328,30 @@ template <class K>
 SIP_HD void sk_mul(int tid, const TileArgs& a, const TileCtx& c, float2* buf) {
     const bool cj = (a.flags & TF_MUL_CONJ) != 0;
     const int total = c.cnt * K::N;
-    for (int f = tid; f < total; f += K::T) {
-        const int q = f / K::N;
-        const int k = f - q * K::N;
-        const float2 m = SIP_LDG(a.mul + (long long)(c.i0 + q) * a.mul_pitch_p + (long long)k * a.mul_pitch_k);
-        float2& v = buf[q * K::LD + K::idx(k)];
-        v = c_mul(v, maybe_conj(m, cj));
+    // B filter values per thread in flight at once: the filter comes from
+    // L2, and one load per iteration would wait out its latency each time
+    constexpr int B = 8;
+    for (int f0 = tid; f0 < total; f0 += B * K::T) {
+        float2 m[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            const int f = f0 + i * K::T;
+            if (f < total) {
+                const int q = f / K::N;
+                const int k = f - q * K::N;
+                m[i] = SIP_LDG(a.mul + (long long)(c.i0 + q) * a.mul_pitch_p + (long long)k * a.mul_pitch_k);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            const int f = f0 + i * K::T;
+            if (f < total) {
+                const int q = f / K::N;
+                const int k = f - q * K::N;
+                float2& v = buf[q * K::LD + K::idx(k)];
+                v = c_mul(v, maybe_conj(m[i], cj));
+            }
+        }
     }
 }
 
@@ -1470,13 +1488,17 @@ __global__ void __launch_bounds__(K::T, K::MINB) sk_fft_kernel(const TileArgs a)
             __syncthreads();
         }
         if constexpr (K::OP == OP_PC) {
-            // forward FFT, filter, inverse FFT, all in shared memory
-            sk_half<SkView<K, OP_PC, -1, false>>(tid, a, c, cur);
-            sk_mul<K>(tid, a, c, cur);
+            // forward FFT, filter, inverse FFT, all in shared memory.  The
+            // butterfly indices and addresses depend on the thread index
+            // alone; opaque copies of it per tile and half keep the
+            // compiler from hoisting them out of the tile loop (fewer
+            // spills: 240 against 328 bytes per thread for 4320 points as
+            // 18 x 16 x 15 on 288 threads)
+            int tid_fwd = tid;
+            asm volatile("" : "+r"(tid_fwd));
+            sk_half<SkView<K, OP_PC, -1, false>>(tid_fwd, a, c, cur);
+            sk_mul<K>(tid_fwd, a, c, cur);
             __syncthreads();
-            // the inverse half's butterfly indices and addresses equal the
-            // forward half's; an opaque copy of the thread index keeps the
-            // compiler from holding them in registers across both halves
             int tid_inv = tid;
             asm volatile("" : "+r"(tid_inv));
             sk_half<SkView<K, OP_C2C, 1, true>>(tid_inv, a, c, cur);
