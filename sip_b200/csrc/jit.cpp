@@ -317,9 +317,12 @@ bool sk_jit_choose(int op, int mode, int sign, bool tw4, int n, long long transf
     if (c.twb < 0 || c.twb > 15) return false;
     if ((c.twb & SK_MIRROR_PAIR) && (!real_op || c.radices.size() < 2)) c.twb &= ~SK_MIRROR_PAIR;
     if ((c.twb & SK_SPLIT_PASS0) && (c.radices.size() < 2 || op == OP_PC)) c.twb &= ~SK_SPLIT_PASS0;
-    const long long tws =
-        (long long)sk_tws_values(op, n, c.radices.data(), (int)c.radices.size(), c.twb) * 8;
     const long long buf = (long long)sk_buffer_values(op, c.P, n, r0) * 8;
+    long long tws = (long long)sk_tws_values(op, n, c.radices.data(), (int)c.radices.size(), c.twb) * 8;
+    if (buf + tws > kMaxTileSmem && (c.twb & SK_TW_SMEM)) {  // no room for the staged twiddles
+        c.twb &= ~SK_TW_SMEM;
+        tws = 0;
+    }
     if (2 * buf + tws <= kMaxTileSmem) c.stages = 2;
     else if (buf + tws <= kMaxTileSmem) c.stages = 1;
     else return false;
@@ -477,7 +480,8 @@ namespace {
 // Candidate configurations of a step, in order of preference: at most 32
 // values per thread and pass (the default), then 16 and 48.
 // SIP_FFT_JIT_E pins one.
-std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, long long transforms) {
+std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, long long transforms,
+                                   size_t* n_first = nullptr) {
     std::vector<int> tries = {32, 16, 48};
     if (env_int("SIP_FFT_JIT_E", 0) > 0) tries = {env_int("SIP_FFT_JIT_E", 0)};
     std::vector<JitCfg> cands;
@@ -498,6 +502,7 @@ std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, 
         orders.push_back(std::vector<int>(orders[0].rbegin(), orders[0].rend()));
     for (size_t oi = 0; oi < orders.size(); ++oi)
     for (int v : tries) {
+        if (oi == 1 && n_first != nullptr && *n_first == 0) *n_first = cands.size();
         JitCfg c;
         if (!sk_jit_choose(op, mode, sign, tw4, n, transforms, &c, v, oi == 0 ? nullptr : &orders[oi])) continue;
         add(c);
@@ -518,6 +523,7 @@ std::vector<JitCfg> jit_candidates(int op, int mode, int sign, bool tw4, int n, 
             if (ok) add(r);
         }
     }
+    if (n_first != nullptr && *n_first == 0) *n_first = cands.size();
     return cands;
 }
 
@@ -528,8 +534,11 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
     // The first candidate in order without register spills wins, else the
     // one with the fewest spilled bytes.  The first is compiled alone (it
     // wins whenever it does not spill, which saves the others' compilation
-    // time); only when it spills are the others compiled, concurrently.
-    const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms);
+    // time); only when it spills are the others of its radix order
+    // compiled, concurrently, and only when they all spill those of the
+    // reversed order.
+    size_t n_first = 0;
+    const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms, &n_first);
     if (cands.empty()) {
         *err = "no run-time configuration for this step";
         return false;
@@ -550,11 +559,17 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
         *out = cands[0];
         return true;
     }
-    std::vector<std::thread> workers;
-    for (size_t i = 1; i < cands.size(); ++i) workers.emplace_back(compile, i);
-    for (auto& w : workers) w.join();
+    auto compile_range = [&](size_t lo, size_t hi) {
+        std::vector<std::thread> workers;
+        for (size_t i = lo; i < hi; ++i) workers.emplace_back(compile, i);
+        for (auto& w : workers) w.join();
+    };
+    compile_range(1, n_first);
+    bool clean = false;
+    for (size_t i = 0; i < n_first; ++i) clean = clean || (res[i].ok && res[i].spill == 0);
+    if (!clean) compile_range(n_first, cands.size());
     int best = -1;
-    for (size_t i = 0; i < cands.size(); ++i) {
+    for (size_t i = 0; i < (clean ? n_first : cands.size()); ++i) {
         if (!res[i].ok) {
             *err = res[i].err;
             continue;

@@ -86,6 +86,7 @@ def test_hint_validation():
 COMPILE_CASES = [
     (OP_C2C, ROWS, -1, 0, 3840, 8192),
     (OP_C2C, ROWS, 1, 0, 2944, 8192),       # radix 23
+    (OP_C2C, ROWS, -1, 0, 16337, 3),        # 17 x 31 x 31: no room for the staged twiddles beside the tile
     (OP_C2C, COLS, -1, 1, 243, 9000),       # four-step column pass with cross twiddles
     (OP_C2C, ROWS_T, 1, 0, 625, 9000),      # four-step row pass, transposed store
     (OP_R2C_HALF, ROWS, -1, 0, 3344, 8192),
