@@ -816,7 +816,10 @@ def run_ours(args) -> None:
             "gflops_2_5nlogn": round(world * step_flops25 / (ms_per_step * 1e-3) / 1e9, 3),
             "hbm_gbs_step": round(world * step_bytes / (ms_per_step * 1e-3) / 1e9, 1),
             "roofline": {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
-                         "traffic": traffic, "kernel": dom["exec"], "kernel_config": dom["kernel"],
+                         "traffic": traffic,
+                         "traffic_source": ("ncu capture of this kernel configuration, scaled to the full launch "
+                                            "by rows (profiles/dram_traffic.md)") if traffic is not None else None,
+                         "kernel": dom["exec"], "kernel_config": dom["kernel"],
                          "algorithmic_bytes": dom["bytes"], "peak_kind": peak_kind},
             "execs": cands,
             "parity": parity,
