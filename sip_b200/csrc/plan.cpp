@@ -1434,7 +1434,9 @@ void build_steps_inner(FftPlan& plan) {
         if (sz[i] > kMaxTileN)
             throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long last = sz[nd - 1];
-    if (c2c ? last > kMaxTileN : !real_fits_tile(last))
+    // C2C: a last axis above one tile, or one that needs Bluestein, runs as
+    // the batched 1-D transform of the rows (four-step or Bluestein)
+    if (!c2c && !real_fits_tile(last))
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long lastc = c2c ? last : last / 2 + 1;  // complex extent of the last axis
     long long rows = b;
@@ -1471,16 +1473,27 @@ void build_steps_inner(FftPlan& plan) {
         st.chunk_per = rows / b;
     };
     if (c2c) {
-        AxisIO io;
-        io.inner = rows;
-        io.in_idist = last;
-        io.out_idist = last;
-        Step st = make_tile_step(OP_C2C, c2c_sign(plan), (int)last, (int)last, false, io, 0, 0,
-                                 "c2c axis " + std::to_string(nd - 1) + " n=" + std::to_string(last));
-        st.src = Loc::In;
-        st.dst = Loc::Out;
-        plan.steps.push_back(st);
-        rows_chunks();
+        if (last <= kMaxTileN && factorizable((int)last, 32)) {
+            AxisIO io;
+            io.inner = rows;
+            io.in_idist = last;
+            io.out_idist = last;
+            Step st = make_tile_step(OP_C2C, c2c_sign(plan), (int)last, (int)last, false, io, 0, 0,
+                                     "c2c axis " + std::to_string(nd - 1) + " n=" + std::to_string(last));
+            st.src = Loc::In;
+            st.dst = Loc::Out;
+            plan.steps.push_back(st);
+            rows_chunks();
+        } else if (c2c_direct(last)) {
+            // the steps of the 1-D plan of `rows` rows (their chunk fields
+            // stay unset, so no multi-D chunk group takes them)
+            C2COpts o;
+            o.src = Loc::In;
+            o.dst = Loc::Out;
+            add_c2c_1d(plan, last, rows, o);
+        } else {
+            add_bluestein(plan, BLUE_C2C, last, rows);
+        }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else if (r2c) {
         add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);

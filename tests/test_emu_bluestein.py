@@ -46,3 +46,23 @@ def test_direct_lengths_do_not_use_bluestein(emu, n):
     x = random_input(O.C2C, [n], 2)
     rc, _, desc = emu_run(emu, O.C2C, O.FORWARD, [n], 2, x)
     assert rc == 0 and "bluestein" not in desc
+
+
+# Multi-dimensional C2C whose contiguous last axis is above one tile (the
+# batched 1-D four-step of the rows) or needs Bluestein, then the column
+# passes of the other axes in place on the destination.
+@pytest.mark.parametrize("sizes,batch", [([4, 20011], 2), ([3, 5, 1009], 1), ([3, 40000], 2), ([2, 3, 65536], 1)])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_multid_large_or_bluestein_last_axis(emu, sizes, batch, direction):
+    x = random_input(O.C2C, sizes, batch, seed=sum(sizes) + batch)
+    rc, out, desc = emu_run(emu, O.C2C, direction, sizes, batch, x)
+    assert rc == 0, desc
+    kinds = [s["what"].split(" n=")[0] for s in json.loads(desc)["steps"]]
+    last = sizes[-1]
+    if last in (20011, 1009):
+        assert any(k.startswith("bluestein") for k in kinds), kinds
+    else:
+        assert kinds[:2] == ["four-step A", "four-step B"], kinds
+    assert kinds[-(len(sizes) - 1):] == [f"c2c axis {ax}" for ax in range(len(sizes) - 2, -1, -1)], kinds
+    err = O.rel_l2(out, O.fp64(O.C2C, direction, x, sizes))
+    assert err <= REL_L2_TOL, err

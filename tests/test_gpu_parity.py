@@ -287,3 +287,13 @@ def test_real_four_step_mirrored_forms(cuda, op, direction, hints, step, n_pair,
     err = O.rel_l2(yt.cpu().numpy(), O.fp64(op, direction, x, [n]))
     h.destroy()
     assert err <= REL_L2_TOL, f"rel_l2 {err:.3e}"
+
+
+# Multi-dimensional C2C whose contiguous last axis is above one tile (the
+# batched 1-D four-step of the rows) or needs Bluestein (prime 20011, and
+# 2053 whose convolution fits one tile), then the column passes.
+@pytest.mark.parametrize("sizes,batch", [([4, 20011], 2), ([3, 5, 2053], 2), ([6, 40000], 2),
+                                         ([2, 3, 65536], 1), ([24, 131072], 1)])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_multid_large_or_bluestein_last_axis(cuda, sizes, batch, direction):
+    _check(cuda, O.C2C, direction, sizes, batch)
