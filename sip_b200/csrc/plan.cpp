@@ -987,7 +987,12 @@ void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
 // is slower than a separate pre-process pass plus the plain four-step
 // (2^20 x 256 rows: 2.12 ms fused, 1.74 ms unfused).  The real-fused planner
 // hint selects either form for both directions.
-void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
+// C2R in a multi-D plan reads its half spectra from `c2r_src` (the column
+// passes' output in the workspace) and puts its own workspace from ws_base.
+void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows, Loc c2r_src = Loc::In,
+                    size_t ws_base = 0) {
+    if (r2c && (c2r_src != Loc::In || ws_base != 0))
+        throw PlanError(ACL_ERROR_INTERNAL_ERROR, "large R2C reads the input");
     if (n % 2 != 0)
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "odd real length " + std::to_string(n) + " above one tile");
     const long long m = n / 2;
@@ -1057,8 +1062,9 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
                 io.out_stride = n2;
                 Step sa = mirrored_step(ea, n1, n2, rows, io, plan.forward() ? TF_CONJ_IN : 0, 2 * m,
                                         "c2r pre + four-step A n=" + std::to_string(n));
-                sa.src = Loc::In;
+                sa.src = c2r_src;
                 sa.dst = Loc::Ws;
+                sa.dst_off = ws_base;
                 plan.steps.push_back(sa);
                 AxisIO b;
                 b.inner = n1;
@@ -1074,10 +1080,11 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
                 sb.L.args.scale = 2.0f;
                 sb.batch_dim = 2;  // the batch rows are the outer index
                 sb.src = Loc::Ws;
+                sb.src_off = ws_base;
                 sb.dst = Loc::Out;
                 plan.steps.push_back(sb);
             }
-            plan.workspace_need = std::max(plan.workspace_need, zbytes);
+            plan.workspace_need = std::max(plan.workspace_need, ws_base + zbytes);
             return;
         }
     }
@@ -1091,7 +1098,7 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     pp.tw2_n = n;
     pp.tw2_count = m + 1;
     C2COpts o;
-    o.scratch_off = 0;
+    o.scratch_off = ws_base;
     if (r2c) {
         pp.real.in_pitch = m;
         pp.real.out_pitch = m + 1;
@@ -1108,20 +1115,20 @@ void add_real_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     } else {
         pp.real.in_pitch = m + 1;
         pp.real.out_pitch = m;
-        pp.src = Loc::In;
+        pp.src = c2r_src;
         pp.dst = Loc::Ws;
-        pp.dst_off = zoff;
+        pp.dst_off = ws_base + zoff;
         pp.what = "c2r pre n=" + std::to_string(n);
         plan.steps.push_back(pp);
         o.sign = 1;
         o.src = Loc::Ws;
-        o.src_off = zoff;
+        o.src_off = ws_base + zoff;
         o.dst = Loc::Out;
         o.last_flags = TF_SCALE;
         o.last_scale = 2.0f;
         add_c2c_1d(plan, m, rows, o);
     }
-    plan.workspace_need = std::max(plan.workspace_need, zoff + zbytes);
+    plan.workspace_need = std::max(plan.workspace_need, ws_base + zoff + zbytes);
 }
 
 }  // namespace
@@ -1435,8 +1442,9 @@ void build_steps_inner(FftPlan& plan) {
             throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long last = sz[nd - 1];
     // C2C: a last axis above one tile, or one that needs Bluestein, runs as
-    // the batched 1-D transform of the rows (four-step or Bluestein)
-    if (!c2c && !real_fits_tile(last))
+    // the batched 1-D transform of the rows (four-step or Bluestein); R2C /
+    // C2R: an even one above one tile as the batched large real transform
+    if (!c2c && !real_fits_tile(last) && (last % 2 != 0 || !real_direct(last)))
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long lastc = c2c ? last : last / 2 + 1;  // complex extent of the last axis
     long long rows = b;
@@ -1496,15 +1504,23 @@ void build_steps_inner(FftPlan& plan) {
         }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else if (r2c) {
-        add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
-        rows_chunks();
+        if (real_fits_tile(last)) {
+            add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
+            rows_chunks();
+        } else {
+            add_real_large(plan, true, last, rows);
+        }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else {
         column_pass(nd - 2, Loc::In, Loc::Ws);
         for (int ax = nd - 3; ax >= 0; --ax) column_pass(ax, Loc::Ws, Loc::Ws);
-        add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
-        rows_chunks();
         plan.workspace_need = (size_t)(rows * lastc * 8);
+        if (real_fits_tile(last)) {
+            add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
+            rows_chunks();
+        } else {
+            add_real_large(plan, false, last, rows, Loc::Ws, (plan.workspace_need + 255) / 256 * 256);
+        }
     }
 }
 

@@ -297,3 +297,11 @@ def test_real_four_step_mirrored_forms(cuda, op, direction, hints, step, n_pair,
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 def test_multid_large_or_bluestein_last_axis(cuda, sizes, batch, direction):
     _check(cuda, O.C2C, direction, sizes, batch)
+
+
+# Multi-dimensional real plans whose even last axis is above one tile.
+@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([12, 1 << 20], 1)])
+@pytest.mark.parametrize("op", [O.R2C, O.C2R])
+@pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
+def test_multid_real_large_last_axis(cuda, sizes, batch, op, direction):
+    _check(cuda, op, direction, sizes, batch)
