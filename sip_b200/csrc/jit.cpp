@@ -536,7 +536,7 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
     // wins whenever it does not spill, which saves the others' compilation
     // time); only when it spills are the others of its radix order
     // compiled, concurrently, and only when they all spill those of the
-    // reversed order.
+    // reversed order (its first alone, then the rest).
     size_t n_first = 0;
     const std::vector<JitCfg> cands = jit_candidates(op, mode, sign, tw4, n, transforms, &n_first);
     if (cands.empty()) {
@@ -567,9 +567,16 @@ bool sk_jit_select(int op, int mode, int sign, bool tw4, int n, long long transf
     compile_range(1, n_first);
     bool clean = false;
     for (size_t i = 0; i < n_first; ++i) clean = clean || (res[i].ok && res[i].spill == 0);
-    if (!clean) compile_range(n_first, cands.size());
+    if (!clean && n_first < cands.size()) {
+        // the reversed order's first candidate alone, then its others
+        compile(n_first);
+        if (!(res[n_first].ok && res[n_first].spill == 0)) compile_range(n_first + 1, cands.size());
+    }
     int best = -1;
-    for (size_t i = 0; i < (clean ? n_first : cands.size()); ++i) {
+    const size_t done = clean ? n_first
+                      : (n_first < cands.size() && res[n_first].ok && res[n_first].spill == 0) ? n_first + 1
+                                                                                           : cands.size();
+    for (size_t i = 0; i < done; ++i) {
         if (!res[i].ok) {
             *err = res[i].err;
             continue;
