@@ -941,7 +941,12 @@ Step mirrored_step(const SkEntry* e, int n, int n_other, long long rows, const A
 // (pass B of the four-step writes back there), then the four-step scratch.
 // The reference takes such lengths whole into its arch35 real core
 // (core/fft/fftcore/fft_r2c_arch35.cpp:121-148).
-void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
+// C2R in a multi-D plan reads its half spectra from `c2r_src` (the column
+// passes' output in the workspace) and puts its own workspace from ws_base.
+void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows, Loc c2r_src = Loc::In,
+                        size_t ws_base = 0) {
+    if (r2c && (c2r_src != Loc::In || ws_base != 0))
+        throw PlanError(ACL_ERROR_INTERNAL_ERROR, "large R2C reads the input");
     const long long pairs = (rows + 1) / 2;
     const size_t zb = ((size_t)(pairs * n * 8) + 255) / 256 * 256;
     const long long h = n / 2 + 1;
@@ -952,15 +957,18 @@ void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     first.pair.in_pitch = r2c ? n : h;
     first.pair.out_pitch = n;
     first.pair.conj = (!r2c && plan.forward()) ? 1 : 0;
-    first.src = Loc::In;
+    first.src = c2r_src;
     first.dst = Loc::Ws;
+    first.dst_off = ws_base;
     first.what = std::string(r2c ? "r2c pair pack" : "c2r pair combine") + " n=" + std::to_string(n);
     plan.steps.push_back(first);
     C2COpts o;
     o.sign = r2c ? -1 : 1;
     o.src = Loc::Ws;
+    o.src_off = ws_base;
     o.dst = Loc::Ws;
-    o.scratch_off = zb;
+    o.dst_off = ws_base;
+    o.scratch_off = ws_base + zb;
     add_c2c_1d(plan, n, pairs, o);
     Step last;
     last.kind = r2c ? StepKind::PairSeparate : StepKind::PairSplit;
@@ -970,10 +978,11 @@ void add_real_odd_large(FftPlan& plan, bool r2c, long long n, long long rows) {
     last.pair.out_pitch = r2c ? h : n;
     last.pair.conj = (r2c && !plan.forward()) ? 1 : 0;
     last.src = Loc::Ws;
+    last.src_off = ws_base;
     last.dst = Loc::Out;
     last.what = std::string(r2c ? "r2c pair separate" : "c2r pair split") + " n=" + std::to_string(n);
     plan.steps.push_back(last);
-    plan.workspace_need = std::max(plan.workspace_need, zb + (size_t)(pairs * n * 8));
+    plan.workspace_need = std::max(plan.workspace_need, ws_base + zb + (size_t)(pairs * n * 8));
 }
 
 // Even real length whose half-length FFT M needs the four-step split.
@@ -1443,8 +1452,9 @@ void build_steps_inner(FftPlan& plan) {
     const long long last = sz[nd - 1];
     // C2C: a last axis above one tile, or one that needs Bluestein, runs as
     // the batched 1-D transform of the rows (four-step or Bluestein); R2C /
-    // C2R: an even one above one tile as the batched large real transform
-    if (!c2c && !real_fits_tile(last) && (last % 2 != 0 || !real_direct(last)))
+    // C2R: one above one tile as the batched large real transform (even:
+    // half length, odd: row pairs through the complex four-step)
+    if (!c2c && !real_fits_tile(last) && !(last % 2 == 0 ? real_direct(last) : c2c_direct(last)))
         throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long lastc = c2c ? last : last / 2 + 1;  // complex extent of the last axis
     long long rows = b;
@@ -1507,8 +1517,10 @@ void build_steps_inner(FftPlan& plan) {
         if (real_fits_tile(last)) {
             add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
             rows_chunks();
-        } else {
+        } else if (last % 2 == 0) {
             add_real_large(plan, true, last, rows);
+        } else {
+            add_real_odd_large(plan, true, last, rows);
         }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else {
@@ -1518,8 +1530,10 @@ void build_steps_inner(FftPlan& plan) {
         if (real_fits_tile(last)) {
             add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
             rows_chunks();
-        } else {
+        } else if (last % 2 == 0) {
             add_real_large(plan, false, last, rows, Loc::Ws, (plan.workspace_need + 255) / 256 * 256);
+        } else {
+            add_real_odd_large(plan, false, last, rows, Loc::Ws, (plan.workspace_need + 255) / 256 * 256);
         }
     }
 }

@@ -68,10 +68,11 @@ def test_multid_large_or_bluestein_last_axis(emu, sizes, batch, direction):
     assert err <= REL_L2_TOL, err
 
 
-# Multi-dimensional real plans whose even last axis is above one tile: the
-# batched large real transform of the rows, then (R2C) or after (C2R) the
-# column passes on the half spectrum.
-@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1)])
+# Multi-dimensional real plans whose last axis is above one tile (even: the
+# half-length transform; odd, 59049 = 3^10: row pairs through the complex
+# four-step), before (R2C) or after (C2R) the column passes on the half
+# spectrum.
+@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([3, 59049], 1), ([2, 2, 59049], 1)])
 @pytest.mark.parametrize("op", [O.R2C, O.C2R])
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 def test_multid_real_large_last_axis(emu, sizes, batch, op, direction):

@@ -299,8 +299,9 @@ def test_multid_large_or_bluestein_last_axis(cuda, sizes, batch, direction):
     _check(cuda, O.C2C, direction, sizes, batch)
 
 
-# Multi-dimensional real plans whose even last axis is above one tile.
-@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([12, 1 << 20], 1)])
+# Multi-dimensional real plans whose last axis is above one tile (even, and
+# odd 59049 = 3^10 through row pairs).
+@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([12, 1 << 20], 1), ([5, 59049], 2)])
 @pytest.mark.parametrize("op", [O.R2C, O.C2R])
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 def test_multid_real_large_last_axis(cuda, sizes, batch, op, direction):
