@@ -806,10 +806,15 @@ void add_bluestein(FftPlan& plan, int kind, long long n, long long batch, const 
 // four-step C2C.  The convolution is half as long as the full-length
 // complex Bluestein's.  Workspace: [0, z) the m-point rows, then the
 // Bluestein's own.
-void add_real_bluestein_half(FftPlan& plan, bool r2c, long long n, long long rows) {
+// C2R in a multi-D plan reads its half spectra from `c2r_src` (the column
+// passes' output in the workspace) and puts its own workspace from ws_base.
+void add_real_bluestein_half(FftPlan& plan, bool r2c, long long n, long long rows, Loc c2r_src = Loc::In,
+                             size_t ws_base = 0) {
+    if (r2c && (c2r_src != Loc::In || ws_base != 0))
+        throw PlanError(ACL_ERROR_INTERNAL_ERROR, "real Bluestein R2C reads the input");
     const long long m = n / 2;
     const size_t zbytes = (size_t)(rows * m * 8);
-    const size_t zoff = (zbytes + 255) / 256 * 256;
+    const size_t zoff = ws_base + (zbytes + 255) / 256 * 256;
     Step pp;
     pp.kind = r2c ? StepKind::RealPost : StepKind::RealPre;
     pp.real.m = m;
@@ -836,14 +841,14 @@ void add_real_bluestein_half(FftPlan& plan, bool r2c, long long n, long long row
     } else {
         pp.real.in_pitch = m + 1;
         pp.real.out_pitch = m;
-        pp.src = Loc::In;
+        pp.src = c2r_src;
         pp.dst = Loc::Ws;
-        pp.dst_off = 0;
+        pp.dst_off = ws_base;
         pp.what = "c2r pre n=" + std::to_string(n);
         plan.steps.push_back(pp);
         io.sign = 1;
         io.src = Loc::Ws;
-        io.src_off = 0;
+        io.src_off = ws_base;
         io.dst = Loc::Out;
         io.scale = 2.0f;
         add_bluestein(plan, BLUE_C2C, m, rows, io);
@@ -1450,12 +1455,18 @@ void build_steps_inner(FftPlan& plan) {
         if (sz[i] > kMaxTileN)
             throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
     const long long last = sz[nd - 1];
-    // C2C: a last axis above one tile, or one that needs Bluestein, runs as
-    // the batched 1-D transform of the rows (four-step or Bluestein); R2C /
-    // C2R: one above one tile as the batched large real transform (even:
-    // half length, odd: row pairs through the complex four-step)
-    if (!c2c && !real_fits_tile(last) && !(last % 2 == 0 ? real_direct(last) : c2c_direct(last)))
-        throw PlanError(ACL_ERROR_API_NOT_SUPPORT, "multi-dimensional axis above one tile is not supported");
+    // A last axis above one tile, or one that needs Bluestein, runs as the
+    // batched 1-D transform of the rows, routed as a 1-D plan of that
+    // length would be: C2C four-step or Bluestein; real: one tile, the
+    // half-length four-step (even), row pairs through the complex four-step
+    // (odd), or Bluestein (half length when even)
+    enum { kRows, kLarge, kOddLarge, kBlueHalf, kBlue };
+    const int real_route = c2c ? kRows
+                         : (real_fits_tile(last) && real_direct(last)) ? kRows
+                         : (last % 2 == 0 && real_direct(last)) ? kLarge
+                         : (last % 2 == 1 && last > kMaxTileN && c2c_direct(last)) ? kOddLarge
+                         : (last % 2 == 0 && last / 2 <= kMaxBluesteinN) ? kBlueHalf
+                                                                           : kBlue;
     const long long lastc = c2c ? last : last / 2 + 1;  // complex extent of the last axis
     long long rows = b;
     for (int i = 0; i < nd - 1; ++i) rows *= sz[i];
@@ -1514,26 +1525,38 @@ void build_steps_inner(FftPlan& plan) {
         }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else if (r2c) {
-        if (real_fits_tile(last)) {
+        if (real_route == kRows) {
             add_real_rows(plan, true, last, rows, Loc::In, Loc::Out);
             rows_chunks();
-        } else if (last % 2 == 0) {
+        } else if (real_route == kLarge) {
             add_real_large(plan, true, last, rows);
-        } else {
+        } else if (real_route == kOddLarge) {
             add_real_odd_large(plan, true, last, rows);
+        } else if (real_route == kBlueHalf) {
+            add_real_bluestein_half(plan, true, last, rows);
+        } else {
+            add_bluestein(plan, BLUE_R2C, last, rows);
         }
         for (int ax = nd - 2; ax >= 0; --ax) column_pass(ax, Loc::Out, Loc::Out);
     } else {
         column_pass(nd - 2, Loc::In, Loc::Ws);
         for (int ax = nd - 3; ax >= 0; --ax) column_pass(ax, Loc::Ws, Loc::Ws);
         plan.workspace_need = (size_t)(rows * lastc * 8);
-        if (real_fits_tile(last)) {
+        const size_t base = (plan.workspace_need + 255) / 256 * 256;
+        if (real_route == kRows) {
             add_real_rows(plan, false, last, rows, Loc::Ws, Loc::Out);
             rows_chunks();
-        } else if (last % 2 == 0) {
-            add_real_large(plan, false, last, rows, Loc::Ws, (plan.workspace_need + 255) / 256 * 256);
+        } else if (real_route == kLarge) {
+            add_real_large(plan, false, last, rows, Loc::Ws, base);
+        } else if (real_route == kOddLarge) {
+            add_real_odd_large(plan, false, last, rows, Loc::Ws, base);
+        } else if (real_route == kBlueHalf) {
+            add_real_bluestein_half(plan, false, last, rows, Loc::Ws, base);
         } else {
-            add_real_odd_large(plan, false, last, rows, Loc::Ws, (plan.workspace_need + 255) / 256 * 256);
+            BlueIO io;
+            io.src = Loc::Ws;
+            io.ws_off = base;
+            add_bluestein(plan, BLUE_C2R, last, rows, io);
         }
     }
 }

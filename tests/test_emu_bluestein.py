@@ -70,9 +70,11 @@ def test_multid_large_or_bluestein_last_axis(emu, sizes, batch, direction):
 
 # Multi-dimensional real plans whose last axis is above one tile (even: the
 # half-length transform; odd, 59049 = 3^10: row pairs through the complex
-# four-step), before (R2C) or after (C2R) the column passes on the half
+# four-step) or needs Bluestein (2018 and 40022 at half length, 1009 at
+# full length), before (R2C) or after (C2R) the column passes on the half
 # spectrum.
-@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([3, 59049], 1), ([2, 2, 59049], 1)])
+@pytest.mark.parametrize("sizes,batch", [([3, 40000], 2), ([2, 3, 65536], 1), ([3, 59049], 1), ([2, 2, 59049], 1),
+                                         ([3, 2018], 2), ([2, 3, 1009], 1), ([5, 40022], 1)])
 @pytest.mark.parametrize("op", [O.R2C, O.C2R])
 @pytest.mark.parametrize("direction", [O.FORWARD, O.INVERSE])
 def test_multid_real_large_last_axis(emu, sizes, batch, op, direction):
